@@ -1,0 +1,205 @@
+/*
+ * omcgpu — C ABI of the B200 dose engine (coupled photon/electron
+ * condensed-history Monte Carlo on voxel phantoms).
+ *
+ * Every entry point returns an int status: OMC_OK (0) or a negative
+ * OMC_E_* code; the message of the last failure of an engine is available
+ * from omc_engine_last_error(), and process-wide failures from
+ * omc_last_error().  Nothing in the library calls exit() or longjmp()
+ * (ompMC exits the process on any error, e.g. ompmc.c:231-234).
+ *
+ * Arrays are plain C arrays owned by the caller; sizes are passed
+ * explicitly.  Voxel arrays are x-fastest: v = i + j*nx + k*nx*ny, which is
+ * ompMC's region number minus one (omc_dosxyz.c:124-128).
+ *
+ * Threading: one host thread drives an engine at a time.
+ */
+#ifndef OMCGPU_H
+#define OMCGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define OMC_OK 0
+#define OMC_E_ARG -1      /* invalid argument */
+#define OMC_E_IO -2       /* file cannot be opened */
+#define OMC_E_FORMAT -3   /* malformed file or data */
+#define OMC_E_MEDIA -4    /* medium missing from the PEGS4 file */
+#define OMC_E_RANGE -5    /* input outside a supported range */
+#define OMC_E_CUDA -10    /* CUDA runtime failure (no device, launch error) */
+#define OMC_E_NOMEM -11   /* device allocation failed / over budget */
+#define OMC_E_DEVICE -12  /* a kernel raised an error flag (see last error) */
+#define OMC_E_BUSY -13    /* serving queue full */
+#define OMC_E_NOTREADY -14 /* request still running */
+
+const char *omc_status_string(int status);
+const char *omc_last_error(void);
+int omc_version(void);
+
+/* ------------------------------------------------------------ tables
+ * Builds every physics table for the named media from a PEGS4 file, the
+ * pgs4form file and a data folder holding xcom_{photo,rayleigh,pair,
+ * triplet}.data, msnew.data and spinms.data.  Replaces ompMC's
+ * initMediaData() (ompmc.c:5468-5503), which reads the same files through
+ * the `.inp` keys `pegs file`, `pgs4form file` and `data folder`.
+ * Host-only: needs no GPU. */
+typedef struct omc_tables omc_tables;
+int omc_tables_build(const char *pegs_file, const char *pgs4form_file, const char *data_folder,
+                     const char *const *media, int nmed, omc_tables **out);
+void omc_tables_free(omc_tables *t);
+/* Read access to a table by ompMC's name (e.g. "gmfp0", "spin_rej",
+ * "range_ep"; the struct fields of ompmc.h:107-406).  *is_int tells whether
+ * *data points at int32 or double. */
+int omc_tables_get(const omc_tables *t, const char *name, const void **data, int64_t *n, int *is_int);
+int omc_tables_nmed(const omc_tables *t);
+
+/* ------------------------------------------------------------ phantom
+ * Rectilinear voxel phantom (omc_dosxyz.c:47-60, omc_matrad.c:364-453).
+ * med: 1-based medium index per voxel (0 = vacuum); rho: g/cm^3. */
+typedef struct {
+    int nx, ny, nz;
+    const double *xb, *yb, *zb; /* nx+1, ny+1, nz+1 boundaries (cm) */
+    const int32_t *med;         /* nx*ny*nz */
+    const double *rho;          /* nx*ny*nz */
+} omc_phantom;
+
+/* ------------------------------------------------------------ engine */
+#define OMC_PLAIN_FP64 0   /* history-based, one thread per history, FP64 */
+#define OMC_EVENT_FP32 1   /* event-based queues, FP32 transport, FP64 tallies */
+
+typedef struct {
+    double ecut;          /* global ecut, total energy (MeV) ("global ecut") */
+    double pcut;          /* global pcut (MeV) ("global pcut") */
+    int device;           /* CUDA device ordinal */
+    int ref_compat;       /* 1: reproduce ompMC's sampling quirks (default) */
+    int64_t queue_capacity; /* event form: particles per queue (0 = default) */
+    int block;            /* threads per block (0 = default) */
+    int nsplit;           /* photon splitting: only 1 is supported */
+} omc_options;
+
+void omc_options_default(omc_options *o);
+
+typedef struct omc_engine omc_engine;
+/* Uploads tables and phantom once; they stay resident across runs. */
+int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_options *o, omc_engine **out);
+int omc_engine_destroy(omc_engine *e);
+const char *omc_engine_last_error(const omc_engine *e);
+
+/* ------------------------------------------------------------ sources */
+/* Energy distribution: a spectrum inverse CDF (cdf1/cdf2 of length n,
+ * omc_dosxyz.c:474-494) or a mono-energetic source (n = 0). */
+typedef struct {
+    int charge;             /* 0 photons, -1 electrons, +1 positrons */
+    double mono_energy;     /* MeV kinetic, when n == 0 */
+    int n;                  /* inverse-CDF size (ompMC: INVDIM = 1000) */
+    const double *cdf1, *cdf2;
+} omc_energy;
+
+/* Reads a `.spectrum` file into an inverse CDF of 1000 points
+ * (omc_dosxyz.c:368-510).  cdf1 and cdf2 must hold 1000 doubles. */
+int omc_spectrum_load(const char *path, double *cdf1, double *cdf2, int *n);
+
+/* Collimated point source on the z axis at distance ssd above the z = zmin
+ * face (omc_dosxyz.c:337-632 and initHistory :964-1068). */
+typedef struct {
+    omc_energy energy;
+    double ssd;
+    double xinl, xinu, yinl, yinu; /* collimator rectangle on the surface */
+} omc_beam;
+
+/* matRad beamlets (omc_matrad.c:618-832, initHistory(ibeamlet) :1177-1413):
+ * a point on the bixel parallelogram corner + r1*side1 + r2*side2, aimed
+ * from the beam's source point (or a Gaussian spot of width gauss_width in
+ * the bixel plane) and traced to the phantom surface. */
+typedef struct {
+    omc_energy energy;
+    int nbeams, nbixels;
+    const int32_t *ibeam;       /* nbixels, 0-based beam of each bixel */
+    const double *src;          /* nbeams*3 */
+    const double *corner;       /* nbixels*3 */
+    const double *side1;        /* nbixels*3 */
+    const double *side2;        /* nbixels*3 */
+    int gaussian;               /* 0 point source, 1 Gaussian spot */
+    double gauss_width;         /* cm */
+} omc_beamlets;
+
+/* --------------------------------------------------- dose runs (dosxyz)
+ * Runs ncase histories (rounded down to nbatch*(ncase/nbatch), as
+ * omc_dosxyz.c:1222-1229) of the beam in `mode`, tallying energy per batch,
+ * and returns dose in Gy per incident particle and the batch-method
+ * relative uncertainty per voxel (accumulateResults, omc_dosxyz.c:719-799,
+ * voxels with rho < 0.044 zeroed).  dose/unc: nvox doubles (may be NULL).
+ * stats (may be NULL) receives [0] histories run, [1] device seconds of the
+ * transport, [2] kernel launches, [3] deposited energy (MeV), [4] source
+ * energy (MeV), [5] error flags. */
+int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, uint64_t seed, int mode,
+                 double *dose, double *unc, double *stats);
+
+/* ------------------------------------------- dose influence (matRad)
+ * One sparse column per beamlet, as the matRad MEX entry builds them
+ * (omc_matrad.c:1576-1720): per beamlet, nhist histories in nbatch
+ * batches, dose in Gy per history (accumEndep divides by the histories of
+ * a batch, omc_matrad.c:897-918), entries above rel_threshold * column
+ * maximum kept, rows = voxel index.  Variance of the mean in var (may be
+ * NULL).  The CSC arrays are caller-owned: colptr has nbixels+1 entries;
+ * rows/vals/var have room for cap entries; *nnz receives the total, and
+ * OMC_E_RANGE is returned (with *nnz the size needed) when cap is short. */
+int omc_run_beamlets(omc_engine *e, const omc_beamlets *b, int64_t nhist, int nbatch, double rel_threshold,
+                     uint64_t seed, int mode, int64_t *colptr, int32_t *rows, double *vals, double *var,
+                     int64_t cap, int64_t *nnz, double *stats);
+
+/* ------------------------------------------------------------ serving
+ * Continuous batching: beam and beamlet requests of any history count are
+ * admitted while device memory for their tallies is within `mem_budget`
+ * bytes, and all admitted requests share the same particle queues.
+ * omc_serve_* replace the sequential beamlet loop of omc_matrad.c:1576. */
+typedef struct omc_server omc_server;
+int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint64_t seed, omc_server **out);
+int omc_server_destroy(omc_server *s);
+/* Submits one beamlet (index ibixel of b, which must outlive the request)
+ * or one beam; returns a request id >= 0 or a negative status. */
+int omc_server_submit_beamlet(omc_server *s, const omc_beamlets *b, int ibixel, int64_t nhist, int nbatch,
+                              double rel_threshold);
+int omc_server_submit_beam(omc_server *s, const omc_beam *b, int64_t nhist, int nbatch);
+/* Advances the device by up to `cycles` transport cycles; *active receives
+ * the requests still running. */
+int omc_server_step(omc_server *s, int cycles, int *active);
+/* Status of a request: OMC_OK when finished, OMC_E_NOTREADY while running. */
+int omc_server_poll(omc_server *s, int id, double *latency_ms);
+/* Sparse column of a finished beamlet request (rows, vals, var of
+ * capacity cap; var may be NULL) or dense dose/unc of a beam request. */
+int omc_server_result_sparse(omc_server *s, int id, int32_t *rows, double *vals, double *var, int64_t cap,
+                             int64_t *nnz);
+int omc_server_result_dense(omc_server *s, int id, double *dose, double *unc);
+int omc_server_release(omc_server *s, int id);
+
+/* ---------------------------------------------- drop-in CLI (dosxyz)
+ * The whole omc_dosxyz program (omc_dosxyz.c:1072-1307): reads
+ * `<inp_base>.inp` (same keys), runs and writes
+ * `<output folder><out_name>.3ddose`.  mode selects the transport form. */
+int omc_dosxyz_run(const char *inp_base, const char *out_name, int mode, int verbose);
+
+/* ------------------------------------------------- validation hooks
+ * Geometry: walks each ray (x,y,z,u,v,w,ir) straight through the phantom
+ * with the FP64 device howfar (omc_dosxyz.c:187-297), recording ustep,
+ * irnew and idisc of every call (up to cap per ray), like the photon
+ * transport loop with an infinite interaction distance.  hownear_out
+ * (nrays, may be NULL) receives hownear at each ray's start. */
+int omc_trace_rays(omc_engine *e, const double *rays, int nrays, int cap, double *ustep, int32_t *irnew,
+                   int32_t *idisc, int32_t *ncalls, double *hownear_out);
+/* Transport: runs history h from primary prim[11*h] (x,y,z,u,v,w,e,wt,
+ * ir,iq,dnear) with the FP64 physics on the scripted uniform stream
+ * rn[rn_off[h] .. rn_off[h+1]), logging every deposit (region, energy)
+ * into dep_ir/dep_e[h*dep_cap ...]; ndep[h] and nused[h] receive the
+ * deposits and random numbers consumed. */
+int omc_replay(omc_engine *e, const double *prim, int nhist, const double *rn, const int64_t *rn_off,
+               int dep_cap, int32_t *dep_ir, double *dep_e, int32_t *ndep, int64_t *nused, uint32_t *flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OMCGPU_H */

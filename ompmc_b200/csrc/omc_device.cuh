@@ -1,0 +1,123 @@
+// Device data model shared by every transport kernel.
+//
+// Tables are interleaved per energy bin so one bin is one or two vector
+// loads: a piecewise-linear table entry is a pair {slope a1, intercept a0},
+// evaluated as a1*lnE + a0 (ompMC pwlfEval, src/ompmc.c:204-212).
+#pragma once
+#include <cstdint>
+
+namespace omc {
+
+#define OMC_HD __host__ __device__ __forceinline__
+
+constexpr int D_MXGE = 2000;
+constexpr int D_MXEKE = 500;
+constexpr int D_MXRAYFF = 100;
+constexpr int D_MXMED = 9;
+constexpr int D_NE1 = 32;       // spin energies
+constexpr int D_NQ1 = 16;       // spin q1 bins
+constexpr int D_NU1 = 32;       // spin u bins
+constexpr int D_NMS = 64 * 8 * 32;
+
+template <typename R>
+struct alignas(2 * sizeof(R)) PL {
+    R a1, a0;
+};
+
+// Photon bin: mean free path, Rayleigh correction, branching ratios.
+template <typename R>
+struct PhBin {
+    PL<R> gmfp, cohe, gbr1, gbr2;
+};
+
+// Electron bin for one charge (0 = e-, 1 = e+).  `range` is the CSDA range
+// from the first grid energy to the bin's lower edge, `earr` that edge.
+template <typename R>
+struct ElBin {
+    PL<R> sig, dedx, tmxs, eta, blcce, q1c, q2c, br1, br2;
+    R range, earr;
+};
+
+template <typename R>
+struct MsE {
+    R u, f, w;
+    int i;
+};
+
+// Per-medium scalars.
+template <typename R>
+struct MedS {
+    R ge0, ge1, eke0, eke1;
+    R blcc, xcc, sige[2];
+    R te, thmoll, ap, ae;
+    R delcm, zbrang, bpar0, bpar1;
+    R pcut, ecut;        // transport cut-offs in this medium
+    R dl1[8], dl2[8], dl3[8], dl4[8], dl5[8], dl6[8];
+    int ismono[2];
+    int meke;
+    int pad;
+};
+
+template <typename R>
+struct Rayl {
+    R xgrid[D_MXRAYFF], fcum[D_MXRAYFF], b[D_MXRAYFF], c[D_MXRAYFF];
+    int ia[D_MXRAYFF];
+};
+
+template <typename R>
+struct DevData {
+    int nmed;
+    int nx, ny, nz;
+    const R *xb, *yb, *zb;          // voxel boundaries
+    const int8_t *med;               // [nvox+1] medium index per region, -1 = vacuum / outside
+    const R *rhof;                   // [nvox+1] density / PEGS density
+    const MedS<R> *ms;               // [nmed]
+    const PhBin<R> *ph;              // [nmed*MXGE]
+    const PL<R> *pmax;               // [nmed*MXGE]
+    const Rayl<R> *ray;              // [nmed]
+    const ElBin<R> *el;              // [(nmed*2)*MXEKE]: (imed*2+qel)*MXEKE + bin
+    const MsE<R> *msurf;             // [NMS]
+    const R *spin;                   // [nmed][2][32][16][32]
+    R b2spin_min, dbeta2i, espml, dleneri, dqq1i, dllambi, dqmsi;
+    int ref_compat;                  // reproduce reference quirks (default 1)
+};
+
+// Beam source of the dosxyz ucode (omc_dosxyz.c:337-632, :964-1068).
+template <typename R>
+struct BeamSrc {
+    int charge;
+    int spectrum;                    // 0 mono, 1 spectrum
+    R energy;
+    const R *cdf1, *cdf2;            // inverse CDF [deltak]
+    R deltak;
+    R ssd, xinl, yinl, xsize, ysize;
+    int ixinl, iyinl;
+};
+
+// Beamlet source of the matRad ucode (omc_matrad.c:1177-1413).
+template <typename R>
+struct BeamletSrc {
+    int charge, spectrum, gaussian;
+    R energy, gauss_width;
+    const R *cdf1, *cdf2;
+    R deltak;
+    // per beamlet
+    const int *ibeam;
+    const R *src;     // [nbeams*3] source position per beam
+    const R *corner;  // [nbixels*3]
+    const R *side1;   // [nbixels*3]
+    const R *side2;   // [nbixels*3]
+};
+
+// Device error flags (or-ed into a word the host reads after each run).
+enum DevErr : unsigned {
+    ERR_STACK = 1u,          // history stack overflow; particle dropped
+    ERR_LOOP = 2u,           // step-count guard tripped; particle dropped
+    ERR_QUEUE = 4u,          // queue overflow; particle dropped
+    ERR_RNG = 8u,            // scripted random stream exhausted
+    ERR_LOG = 16u,           // deposit log full
+    ERR_LAMBDA = 32u,        // BCA lambda_max <= 0; particle dropped (as the reference)
+    ERR_NAN = 64u,           // non-finite state; particle dropped
+};
+
+}  // namespace omc

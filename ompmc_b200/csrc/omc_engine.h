@@ -1,0 +1,78 @@
+// Internal engine state shared by the translation units of libomcgpu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "omc_device.cuh"
+#include "omc_host.h"
+#include "../../include/omcgpu.h"
+
+struct omc_tables {
+    omc::Tables t;
+};
+
+namespace omc {
+
+// Device allocation with ownership.
+struct DBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    int alloc(size_t bytes);
+    template <typename T>
+    T *as() const { return (T *)p; }
+};
+
+// One precision's worth of resident device tables and geometry.
+template <typename R>
+struct DevSet {
+    DBuf xb, yb, zb, med, rhof, ms, ph, pmax, ray, el, msurf, spin;
+    DevData<R> d{};
+};
+
+struct KernelStats {
+    double seconds = 0;     // device time of the transport kernels
+    long launches = 0;      // kernel launches in the transport
+    unsigned flags = 0;     // DevErr bits
+};
+
+}  // namespace omc
+
+struct omc_engine {
+    omc::Tables tabs;
+    omc::Phantom ph;
+    omc::Regions reg;
+    omc_options opt{};
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    omc::DevSet<double> d64;
+    omc::DevSet<float> d32;
+    omc::DBuf rho_vox;      // FP64 density per voxel (dose conversion)
+    omc::DBuf errword;      // unsigned device error flags
+    std::string err;
+    std::vector<double> mass;  // voxel mass (g), host copy
+    omc::DBuf mass_d;
+};
+
+namespace omc {
+int set_err(omc_engine *e, int code, const std::string &msg);
+int cuda_check(omc_engine *e, cudaError_t rc, const char *what);
+
+// Plain FP64 form (omc_plain.cu).
+int plain_beam_batch(omc_engine *e, const BeamSrc<double> &S, double *work, uint64_t seed, long hist0, long n,
+                     double *src_energy, int block);
+int plain_beamlet_batch(omc_engine *e, const BeamletSrc<double> &S, int ib, double *work, uint64_t seed, long hist0,
+                        long n, int block);
+int plain_trace(omc_engine *e, const double *rays_d, int nrays, int cap, double *ustep, int *irnew, int *idisc,
+                int *ncalls, double *hn);
+int plain_replay(omc_engine *e, const double *prim, int nhist, const double *rn, const long *rn_off, int dep_cap,
+                 int *dep_ir, double *dep_e, int *ndep, long *nused, unsigned *flags);
+}  // namespace omc

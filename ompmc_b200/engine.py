@@ -1,0 +1,322 @@
+"""Python host mirror of the engine's C ABI (include/omcgpu.h).
+
+Mirrors ompMC's two surfaces for the transport path:
+
+* `dosxyz(inp_base, out_name)` is the omc_dosxyz program
+  (ucodes/omc_dosxyz/omc_dosxyz.c:1072-1307): same `.inp` keys, writes the
+  same `.3ddose` file;
+* `matrad_dij(cubeRho, cubeMatIx, mcGeo, mcSrc, mcOpt)` is the matRad MEX
+  entry (ucodes/omc_matrad/omc_matrad.c:1417-1789): same inputs (dicts in
+  place of MATLAB structs), returns scipy CSC matrices D (and V).
+
+Errors raise `OmcError` carrying the library's status and message (the
+reference calls exit() or mexErrMsgIdAndTxt).  The library is loaded from the
+package directory; there is no fallback when it is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libomcgpu.so"
+CLI_PATH = PKG / "bin" / "omc_dosxyz"
+
+PLAIN_FP64 = 0
+EVENT_FP32 = 1
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+_up = C.POINTER(C.c_uint32)
+
+
+class OmcError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+class _Phantom(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("xb", _dp), ("yb", _dp), ("zb", _dp), ("med", _ip), ("rho", _dp)]
+
+
+class _Options(C.Structure):
+    _fields_ = [("ecut", C.c_double), ("pcut", C.c_double), ("device", C.c_int),
+                ("ref_compat", C.c_int), ("queue_capacity", C.c_int64), ("block", C.c_int),
+                ("nsplit", C.c_int)]
+
+
+class _Energy(C.Structure):
+    _fields_ = [("charge", C.c_int), ("mono_energy", C.c_double), ("n", C.c_int),
+                ("cdf1", _dp), ("cdf2", _dp)]
+
+
+class _Beam(C.Structure):
+    _fields_ = [("energy", _Energy), ("ssd", C.c_double), ("xinl", C.c_double),
+                ("xinu", C.c_double), ("yinl", C.c_double), ("yinu", C.c_double)]
+
+
+class _Beamlets(C.Structure):
+    _fields_ = [("energy", _Energy), ("nbeams", C.c_int), ("nbixels", C.c_int),
+                ("ibeam", _ip), ("src", _dp), ("corner", _dp), ("side1", _dp), ("side2", _dp),
+                ("gaussian", C.c_int), ("gauss_width", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libomcgpu.so (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise OmcError(-2, f"{LIB_PATH} is not built; run `make -C {PKG}`")
+    L = C.CDLL(str(LIB_PATH))
+    sig = {
+        "omc_status_string": ([C.c_int], C.c_char_p),
+        "omc_last_error": ([], C.c_char_p),
+        "omc_version": ([], C.c_int),
+        "omc_tables_build": ([C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_char_p), C.c_int,
+                              C.POINTER(C.c_void_p)], C.c_int),
+        "omc_tables_free": ([C.c_void_p], None),
+        "omc_tables_get": ([C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p), _lp, C.POINTER(C.c_int)], C.c_int),
+        "omc_tables_nmed": ([C.c_void_p], C.c_int),
+        "omc_spectrum_load": ([C.c_char_p, _dp, _dp, C.POINTER(C.c_int)], C.c_int),
+        "omc_options_default": ([C.POINTER(_Options)], None),
+        "omc_engine_create": ([C.c_void_p, C.POINTER(_Phantom), C.POINTER(_Options), C.POINTER(C.c_void_p)], C.c_int),
+        "omc_engine_destroy": ([C.c_void_p], C.c_int),
+        "omc_engine_last_error": ([C.c_void_p], C.c_char_p),
+        "omc_run_beam": ([C.c_void_p, C.POINTER(_Beam), C.c_int64, C.c_int, C.c_uint64, C.c_int, _dp, _dp, _dp],
+                         C.c_int),
+        "omc_run_beamlets": ([C.c_void_p, C.POINTER(_Beamlets), C.c_int64, C.c_int, C.c_double, C.c_uint64, C.c_int,
+                              _lp, _ip, _dp, _dp, C.c_int64, _lp, _dp], C.c_int),
+        "omc_dosxyz_run": ([C.c_char_p, C.c_char_p, C.c_int, C.c_int], C.c_int),
+        "omc_trace_rays": ([C.c_void_p, _dp, C.c_int, C.c_int, _dp, _ip, _ip, _ip, _dp], C.c_int),
+        "omc_replay": ([C.c_void_p, _dp, C.c_int, _dp, _lp, C.c_int, _ip, _dp, _ip, _lp, _up], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name, None)
+        if f is None:
+            continue
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _check(rc, eng=None):
+    if rc != 0:
+        L = lib()
+        msg = (L.omc_engine_last_error(eng) if eng else L.omc_last_error()) or b""
+        raise OmcError(rc, msg.decode(errors="replace") or L.omc_status_string(rc).decode())
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+class Tables:
+    """Physics tables for the named media (initMediaData, ompmc.c:5468)."""
+
+    def __init__(self, pegs_file, pgs4form_file, data_folder, media):
+        L = lib()
+        self.media = list(media)
+        arr = (C.c_char_p * len(media))(*[m.encode() for m in media])
+        h = C.c_void_p()
+        data_folder = str(data_folder)
+        if not data_folder.endswith("/"):
+            data_folder += "/"
+        _check(L.omc_tables_build(str(pegs_file).encode(), str(pgs4form_file).encode(), data_folder.encode(),
+                                  arr, len(media), C.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_assets(cls, media, root=None):
+        from . import assets
+        root = Path(root) if root else assets.require_assets()
+        return cls(root / "pegs4" / "521icru.pegs4dat", root / "pegs4" / "pgs4form.dat", root / "data", media)
+
+    def get(self, name):
+        L = lib()
+        ptr = C.c_void_p()
+        n = C.c_int64()
+        is_int = C.c_int()
+        _check(L.omc_tables_get(self.h, name.encode(), C.byref(ptr), C.byref(n), C.byref(is_int)))
+        if n.value == 0:
+            return np.zeros(0)
+        t = _ip if is_int.value else _dp
+        return np.ctypeslib.as_array(C.cast(ptr, t), shape=(n.value,)).copy()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().omc_tables_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def load_spectrum(path):
+    """Inverse CDF of a `.spectrum` file (omc_dosxyz.c:368-510)."""
+    c1 = np.zeros(1000)
+    c2 = np.zeros(1000)
+    n = C.c_int()
+    _check(lib().omc_spectrum_load(str(path).encode(), _p(c1, _dp), _p(c2, _dp), C.byref(n)))
+    return c1[:n.value], c2[:n.value]
+
+
+class Engine:
+    """Resident tables + phantom on one GPU."""
+
+    def __init__(self, tables: Tables, phantom, ecut=0.7, pcut=0.01, device=0, ref_compat=True,
+                 queue_capacity=0, block=0):
+        L = lib()
+        self.tables = tables
+        self.phantom = phantom
+        self._xb = np.ascontiguousarray(phantom.xb, dtype=np.float64)
+        self._yb = np.ascontiguousarray(phantom.yb, dtype=np.float64)
+        self._zb = np.ascontiguousarray(phantom.zb, dtype=np.float64)
+        self._med = np.ascontiguousarray(phantom.med, dtype=np.int32).ravel()
+        self._rho = np.ascontiguousarray(phantom.rho, dtype=np.float64).ravel()
+        nx, ny, nz = phantom.shape
+        self.shape = (nz, ny, nx)
+        P = _Phantom(nx, ny, nz, _p(self._xb, _dp), _p(self._yb, _dp), _p(self._zb, _dp),
+                     _p(self._med, _ip), _p(self._rho, _dp))
+        o = _Options()
+        L.omc_options_default(C.byref(o))
+        o.ecut, o.pcut, o.device = ecut, pcut, device
+        o.ref_compat = 1 if ref_compat else 0
+        o.queue_capacity = queue_capacity
+        o.block = block
+        h = C.c_void_p()
+        _check(L.omc_engine_create(tables.h, C.byref(P), C.byref(o), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().omc_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _energy(spectrum=None, mono_energy=1.25, charge=0, keep=None):
+        e = _Energy()
+        e.charge = charge
+        e.mono_energy = mono_energy
+        if spectrum is not None:
+            c1, c2 = (np.ascontiguousarray(a, dtype=np.float64) for a in spectrum)
+            keep += [c1, c2]
+            e.n = len(c1)
+            e.cdf1, e.cdf2 = _p(c1, _dp), _p(c2, _dp)
+        return e
+
+    def run_beam(self, ncase, nbatch=10, seed=1, mode=EVENT_FP32, spectrum=None, mono_energy=1.25, charge=0,
+                 ssd=100.0, collimator=(-5.0, 5.0, -5.0, 5.0)):
+        """Dose (Gy per history) and relative uncertainty arrays [nz,ny,nx]
+        plus a stats dict; the dosxyz beam source (omc_dosxyz.c:964-1068)."""
+        keep = []
+        b = _Beam()
+        b.energy = self._energy(spectrum, mono_energy, charge, keep)
+        b.ssd = ssd
+        b.xinl, b.xinu, b.yinl, b.yinu = collimator
+        n = int(np.prod(self.shape))
+        dose = np.zeros(n)
+        unc = np.zeros(n)
+        st = np.zeros(6)
+        _check(lib().omc_run_beam(self.h, C.byref(b), int(ncase), int(nbatch), int(seed) & (2**64 - 1), mode,
+                                  _p(dose, _dp), _p(unc, _dp), _p(st, _dp)), self.h)
+        stats = dict(histories=st[0], seconds=st[1], launches=int(st[2]), edep=st[3], esrc=st[4],
+                     flags=int(st[5]))
+        return dose.reshape(self.shape), unc.reshape(self.shape), stats
+
+    def run_beamlets(self, beamlets: dict, nhist, nbatch=10, rel_threshold=1e-4, seed=1, mode=EVENT_FP32,
+                     with_variance=True):
+        """matRad D_ij columns (omc_matrad.c:1576-1720) as CSC arrays."""
+        keep = []
+        b = self._beamlets_struct(beamlets, keep)
+        nb = b.nbixels
+        cap = int(beamlets.get("cap", max(1, int(np.prod(self.shape)) * nb // 20 + 1024)))
+        for _ in range(3):
+            colptr = np.zeros(nb + 1, dtype=np.int64)
+            rows = np.zeros(cap, dtype=np.int32)
+            vals = np.zeros(cap)
+            var = np.zeros(cap) if with_variance else None
+            nnz = C.c_int64()
+            st = np.zeros(6)
+            rc = lib().omc_run_beamlets(self.h, C.byref(b), int(nhist), int(nbatch), float(rel_threshold),
+                                        int(seed), mode, _p(colptr, _lp), _p(rows, _ip), _p(vals, _dp),
+                                        _p(var, _dp) if var is not None else None, cap, C.byref(nnz),
+                                        _p(st, _dp))
+            if rc == -5 and nnz.value > cap:
+                cap = nnz.value
+                continue
+            _check(rc, self.h)
+            k = nnz.value
+            stats = dict(histories=st[0], seconds=st[1], launches=int(st[2]), flags=int(st[5]))
+            return colptr, rows[:k], vals[:k], (var[:k] if var is not None else None), stats
+        raise OmcError(-5, "sparse capacity kept growing")
+
+    @staticmethod
+    def _beamlets_struct(bl, keep):
+        b = _Beamlets()
+        b.energy = Engine._energy(bl.get("spectrum"), bl.get("mono_energy", 1.25), bl.get("charge", 0), keep)
+        ibeam = np.ascontiguousarray(bl["ibeam"], dtype=np.int32)
+        src = np.ascontiguousarray(bl["src"], dtype=np.float64).reshape(-1, 3)
+        corner = np.ascontiguousarray(bl["corner"], dtype=np.float64).reshape(-1, 3)
+        s1 = np.ascontiguousarray(bl["side1"], dtype=np.float64).reshape(-1, 3)
+        s2 = np.ascontiguousarray(bl["side2"], dtype=np.float64).reshape(-1, 3)
+        keep += [ibeam, src, corner, s1, s2]
+        b.nbeams, b.nbixels = len(src), len(corner)
+        b.ibeam, b.src, b.corner = _p(ibeam, _ip), _p(src, _dp), _p(corner, _dp)
+        b.side1, b.side2 = _p(s1, _dp), _p(s2, _dp)
+        b.gaussian = 1 if bl.get("gaussian") else 0
+        b.gauss_width = float(bl.get("gauss_width", 0.2123))
+        return b
+
+    # ------------------------------------------------ validation hooks
+    def trace_rays(self, rays, cap=512):
+        """FP64 device howfar walk per ray (x,y,z,u,v,w,ir)."""
+        rays = np.ascontiguousarray(rays, dtype=np.float64)
+        nr = len(rays)
+        us = np.zeros((nr, cap))
+        irn = np.zeros((nr, cap), dtype=np.int32)
+        idc = np.zeros((nr, cap), dtype=np.int32)
+        nc = np.zeros(nr, dtype=np.int32)
+        hn = np.zeros(nr)
+        _check(lib().omc_trace_rays(self.h, _p(rays, _dp), nr, cap, _p(us, _dp), _p(irn, _ip), _p(idc, _ip),
+                                    _p(nc, _ip), _p(hn, _dp)), self.h)
+        return us, irn, idc, nc, hn
+
+    def replay(self, prim, rn, rn_off, dep_cap=2048):
+        """FP64 histories on recorded uniform streams; per-history deposits."""
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        rn = np.ascontiguousarray(rn, dtype=np.float64)
+        rn_off = np.ascontiguousarray(rn_off, dtype=np.int64)
+        nh = len(prim)
+        dir_ = np.zeros((nh, dep_cap), dtype=np.int32)
+        de = np.zeros((nh, dep_cap))
+        nd = np.zeros(nh, dtype=np.int32)
+        nu = np.zeros(nh, dtype=np.int64)
+        fl = np.zeros(nh, dtype=np.uint32)
+        _check(lib().omc_replay(self.h, _p(prim, _dp), nh, _p(rn, _dp), _p(rn_off, _lp), dep_cap, _p(dir_, _ip),
+                                _p(de, _dp), _p(nd, _ip), _p(nu, _lp), _p(fl, _up)), self.h)
+        return dir_, de, nd, nu, fl
+
+
+def dosxyz(inp_base, out_name, mode=EVENT_FP32, verbose=False):
+    """The omc_dosxyz program: `<inp_base>.inp` in, `.3ddose` out."""
+    _check(lib().omc_dosxyz_run(str(inp_base).encode(), str(out_name).encode(), mode, 1 if verbose else 0))

@@ -1,0 +1,167 @@
+"""Generates the golden fixtures in this directory from the unmodified
+reference (built by oracle/Makefile) — run here, where an ompMC checkout
+exists; the fixtures are committed so GPU hosts need neither.
+
+    python tests/golden/make_golden.py [--only NAME]
+
+Fixtures (all seeded; reference RNG seeds 97 33, one thread):
+  rays_<case>.npz     random rays and the reference howfar walk of each
+                      (ustep, irnew, idisc per call) and hownear at start
+  replay_<case>.npz   primaries, the uniform stream each history consumed
+                      (stored exactly as integers rn * 2^24, RANMAR's
+                      resolution) and its deposit sequence (region, energy)
+  dose_<case>.npz     reference CLI dose and relative uncertainty of the
+                      voxels above 5 % of the maximum (8 threads, 2e6 histories in 50 batches)
+  (the table comparison runs against the live oracle; no fixture)
+Cases: water30 (30^3 x 1 cm water), slab64 (64^3 x 0.25 cm water/lung/bone),
+ctsmall (32x32x24 x 1.2 cm CT-like, 4 media).
+"""
+from __future__ import annotations
+
+import argparse
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent.parent
+sys.path.insert(0, str(REPO))
+
+from ompmc_b200 import assets as A  # noqa: E402
+
+WORK = REPO / "assets" / "golden_work"
+
+CASES = {
+    "water30": dict(phantom=lambda: A.water_cube(30, 1.0), collimator=(-5, 5, -5, 5)),
+    "slab64": dict(phantom=lambda: A.slab_phantom(64, 0.25), collimator=(-2.5, 2.5, -2.5, 2.5)),
+    "ctsmall": dict(phantom=lambda: A.ct_phantom(32, 32, 24, 1.2, seed=7), collimator=(-5, 5, -5, 5)),
+}
+
+TABLES = ["ge0", "ge1", "gmfp0", "gmfp1", "gbr10", "gbr11", "gbr20", "gbr21", "cohe0", "cohe1", "xgrid", "fcum",
+          "b_array", "c_array", "pmax0", "pmax1", "i_array", "dl1", "dl2", "dl3", "dl4", "dl5", "dl6", "bpar0",
+          "bpar1", "delcm", "zbrang", "esig0", "esig1", "psig0", "psig1", "ededx0", "ededx1", "pdedx0", "pdedx1",
+          "ebr10", "ebr11", "pbr10", "pbr11", "pbr20", "pbr21", "tmxs0", "tmxs1", "blcce0", "blcce1", "etae_ms0",
+          "etae_ms1", "etap_ms0", "etap_ms1", "q1ce_ms0", "q1ce_ms1", "q1cp_ms0", "q1cp_ms1", "q2ce_ms0",
+          "q2ce_ms1", "q2cp_ms0", "q2cp_ms1", "range_ep", "e_array", "eke0", "eke1", "sig_ismonotone", "esig_e",
+          "psig_e", "xcc", "blcc", "expeke1", "spin_rej", "ums", "fms", "wms", "ims", "meke"]
+
+
+def case_inp(name, ncase=100000, nbatch=10):
+    """Phantom + spectrum + `.inp` of a case under assets/golden_work."""
+    A.require_assets()
+    c = CASES[name]
+    ph = c["phantom"]()
+    pf = WORK / f"{name}.egsphant"
+    if not pf.exists():
+        A.write_egsphant(pf, ph)
+    run = A.default_run(pf, ncase=ncase, nbatch=nbatch, collimator=c["collimator"])
+    base = WORK / f"{name}_{ncase}"
+    A.write_inp(base, run)
+    return base, ph
+
+
+def random_rays(ph, n, rng):
+    """Rays starting inside random voxels, isotropic directions."""
+    nx, ny, nz = ph.shape
+    i = rng.integers(0, nx, n)
+    j = rng.integers(0, ny, n)
+    k = rng.integers(0, nz, n)
+    fx, fy, fz = rng.random((3, n))
+    x = ph.xb[i] + fx * (ph.xb[i + 1] - ph.xb[i])
+    y = ph.yb[j] + fy * (ph.yb[j + 1] - ph.yb[j])
+    z = ph.zb[k] + fz * (ph.zb[k + 1] - ph.zb[k])
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    # a few axis-aligned rays exercise the zero-cosine branches
+    d[: n // 10] = np.eye(3)[rng.integers(0, 3, n // 10)] * rng.choice([-1, 1], (n // 10, 1))
+    ir = 1 + i + j * nx + k * nx * ny
+    return np.column_stack([x, y, z, d, ir]).astype(np.float64)
+
+
+def _in_subprocess(name, what, out):
+    """The reference keeps global state: one configuration per process."""
+    code = (f"import sys; sys.path.insert(0, {str(REPO)!r}); sys.argv=['x']; "
+            f"from tests.golden import make_golden as M; M._{what}({name!r}, {str(out)!r})")
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
+    if p.returncode != 0:
+        raise RuntimeError(p.stdout[-3000:] + p.stderr[-3000:])
+
+
+def _rays(name, out):
+    from oracle.ref import Reference
+    base, ph = case_inp(name)
+    r = Reference.open(base)
+    rays = random_rays(ph, 300, np.random.default_rng(11))
+    cap = 4 * sum(ph.shape)
+    us = np.zeros((len(rays), cap))
+    irn = np.zeros((len(rays), cap), dtype=np.int32)
+    idc = np.zeros((len(rays), cap), dtype=np.int32)
+    nc = np.zeros(len(rays), dtype=np.int32)
+    hn = np.zeros(len(rays))
+    for q, ray in enumerate(rays):
+        a, b, c = r.walk(*ray[:6], int(ray[6]), cap=cap)
+        n = len(a)
+        us[q, :n], irn[q, :n], idc[q, :n], nc[q] = a, b, c, n
+        hn[q] = r.hownear(*ray[:3], int(ray[6]))
+    np.savez_compressed(out, rays=rays, ustep=us, irnew=irn, idisc=idc, ncalls=nc, hownear=hn, cap=cap)
+
+
+def _replay(name, out):
+    from oracle.ref import Reference
+    base, _ = case_inp(name)
+    r = Reference.open(base)
+    nh = {"water30": 200, "slab64": 150, "ctsmall": 150}[name]
+    res = r.run(nh)
+    rn_int = np.round(res["rn"] * 16777216.0).astype(np.uint32)
+    assert np.array_equal(rn_int.astype(np.float64) / 16777216.0, res["rn"])
+    np.savez_compressed(out, prim=res["prim"], rn_int=rn_int, rn_off=res["rn_off"], dep_ir=res["dep_ir"],
+                        dep_e=res["dep_e"], d_off=res["d_off"])
+
+
+def _tables(name, out):
+    from oracle.ref import Reference
+    base, _ = case_inp(name)
+    r = Reference.open(base)
+    d = {n: r.table(n) for n in TABLES}
+    for k, v in r.spin_scalars().items():
+        d["s_" + k] = np.array(v)
+    np.savez_compressed(out, **d)
+
+
+def make_dose(name, ncase=2000000, nbatch=50, cores=8):
+    from oracle.ref import run_cli
+    base, ph = case_inp(name, ncase=ncase, nbatch=nbatch)
+    loop_s, _ = run_cli(base, f"golden_{name}", cores=cores)
+    dose, unc, _ = A.read_3ddose(A.ASSETS / "out" / f"golden_{name}.3ddose")
+    keep = np.flatnonzero(dose.ravel() > 0.05 * dose.max())
+    np.savez_compressed(HERE / f"dose_{name}.npz", idx=keep.astype(np.int32), dose=dose.ravel()[keep],
+                        unc=unc.ravel()[keep].astype(np.float32), shape=np.array(dose.shape), dmax=dose.max(),
+                        ncase=ncase, nbatch=nbatch, loop_seconds=loop_s, cores=cores)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", default=None)
+    a = ap.parse_args()
+    from oracle.ref import build
+    build()
+    A.require_assets()
+    WORK.mkdir(parents=True, exist_ok=True)
+    jobs = [("rays", n) for n in CASES] + [("replay", n) for n in CASES]
+    for what, name in jobs:
+        fn = f"{what}_{name}"
+        if a.only and a.only not in fn:
+            continue
+        print("generating", fn, flush=True)
+        _in_subprocess(name, what, HERE / f"{fn}.npz")
+    for name in ("water30", "slab64"):
+        if a.only and a.only not in f"dose_{name}":
+            continue
+        print("generating dose", name, flush=True)
+        make_dose(name)
+
+
+if __name__ == "__main__":
+    main()
