@@ -230,7 +230,9 @@ class Phantom:
 
 
 def _grid(n, d, lo):
-    return lo + d * np.arange(n + 1, dtype=np.float64)
+    """Boundaries rounded to the 6 decimals of the `.egsphant` text, so the
+    arrays handed to the engine equal what a reader of the file gets."""
+    return np.round(lo + d * np.arange(n + 1, dtype=np.float64), 6)
 
 
 def water_cube(n=30, d=1.0):
@@ -288,6 +290,7 @@ def ct_phantom(nx=128, ny=128, nz=96, d=0.3, seed=1234, scale=(1.0, 1.0, 1.0)):
     spine = (X / (1.5 * sx)) ** 2 + ((Y + 7.0 * sy) / (1.5 * sx)) ** 2 <= 1.0
     spine &= body
     rho[spine] = rng.uniform(1.4, 1.9, size=int(spine.sum()))
+    rho = np.round(rho, 6)
     med = np.digitize(rho, CT_THRESHOLDS).astype(np.int32) + 1
     return Phantom(list(CT_MEDIA), xb, yb, zb, med, rho, name=f"ct{nx}x{ny}x{nz}")
 

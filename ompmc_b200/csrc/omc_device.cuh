@@ -8,7 +8,9 @@
 
 namespace omc {
 
+#ifndef OMC_HD
 #define OMC_HD __host__ __device__ __forceinline__
+#endif
 
 constexpr int D_MXGE = 2000;
 constexpr int D_MXEKE = 500;

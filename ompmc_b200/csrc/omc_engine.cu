@@ -64,43 +64,38 @@ static PL<R> mkpl(double a1, double a0) {
     return p;
 }
 
-// Host tables -> interleaved device layout in precision R.
+// Host tables -> interleaved device layout in precision R (host vectors).
 template <typename R>
-static int build_devset(omc_engine *e, DevSet<R> &S) {
-    const Tables &t = e->tabs;
-    const Phantom &ph = e->ph;
-    const Regions &rg = e->reg;
+void make_layout(const Tables &t, const Phantom &ph, const Regions &rg, double ecut, double pcut, int ref_compat,
+                 Layout<R> &L) {
     int nmed = t.nmed;
-    DevData<R> &d = S.d;
+    DevData<R> &d = L.d;
+    d = DevData<R>{};
     d.nmed = nmed;
     d.nx = ph.nx;
     d.ny = ph.ny;
     d.nz = ph.nz;
-    d.ref_compat = e->opt.ref_compat;
-    int rc;
-    auto cvt = [](const std::vector<double> &v) { return std::vector<R>(v.begin(), v.end()); };
-    if ((rc = upload(e, S.xb, cvt(ph.xb)))) return rc;
-    if ((rc = upload(e, S.yb, cvt(ph.yb)))) return rc;
-    if ((rc = upload(e, S.zb, cvt(ph.zb)))) return rc;
-    std::vector<int8_t> med(rg.med.begin(), rg.med.end());
-    if ((rc = upload(e, S.med, med))) return rc;
-    if ((rc = upload(e, S.rhof, cvt(rg.rhof)))) return rc;
-
-    std::vector<MedS<R>> ms(nmed);
-    std::vector<PhBin<R>> phb((size_t)nmed * D_MXGE);
-    std::vector<PL<R>> pmax((size_t)nmed * D_MXGE);
-    std::vector<Rayl<R>> ray(nmed);
-    std::vector<ElBin<R>> el((size_t)nmed * 2 * D_MXEKE);
+    d.ref_compat = ref_compat;
+    L.xb.assign(ph.xb.begin(), ph.xb.end());
+    L.yb.assign(ph.yb.begin(), ph.yb.end());
+    L.zb.assign(ph.zb.begin(), ph.zb.end());
+    L.med.assign(rg.med.begin(), rg.med.end());
+    L.rhof.assign(rg.rhof.begin(), rg.rhof.end());
+    L.ms.assign(nmed, MedS<R>{});
+    L.ph.assign((size_t)nmed * D_MXGE, PhBin<R>{});
+    L.pmax.assign((size_t)nmed * D_MXGE, PL<R>{});
+    L.ray.assign(nmed, Rayl<R>{});
+    L.el.assign((size_t)nmed * 2 * D_MXEKE, ElBin<R>{});
     for (int im = 0; im < nmed; im++) {
         const PegsMedium &m = t.pegs[im];
-        MedS<R> &s = ms[im];
+        MedS<R> &s = L.ms[im];
         std::memset(&s, 0, sizeof(s));
         s.ge0 = t.ge0[im]; s.ge1 = t.ge1[im]; s.eke0 = t.eke0[im]; s.eke1 = t.eke1[im];
         s.blcc = t.blcc[im]; s.xcc = t.xcc[im]; s.sige[0] = t.esig_e[im]; s.sige[1] = t.psig_e[im];
         s.te = m.te; s.thmoll = m.thmoll; s.ap = m.ap; s.ae = m.ae;
         s.delcm = t.delcm[im]; s.zbrang = t.zbrang[im]; s.bpar0 = t.bpar0[im]; s.bpar1 = t.bpar1[im];
-        s.pcut = m.ap <= e->opt.pcut ? e->opt.pcut : m.ap;
-        s.ecut = m.ae <= e->opt.ecut ? e->opt.ecut : m.ae;
+        s.pcut = m.ap <= pcut ? pcut : m.ap;
+        s.ecut = m.ae <= ecut ? ecut : m.ae;
         for (int k = 0; k < 8; k++) {
             s.dl1[k] = t.dl1[im * 8 + k]; s.dl2[k] = t.dl2[im * 8 + k]; s.dl3[k] = t.dl3[im * 8 + k];
             s.dl4[k] = t.dl4[im * 8 + k]; s.dl5[k] = t.dl5[im * 8 + k]; s.dl6[k] = t.dl6[im * 8 + k];
@@ -110,25 +105,25 @@ static int build_devset(omc_engine *e, DevSet<R> &S) {
         s.meke = m.meke;
         for (int j = 0; j < D_MXGE; j++) {
             size_t o = (size_t)im * D_MXGE + j;
-            PhBin<R> &b = phb[o];
+            PhBin<R> &b = L.ph[o];
             b.gmfp = mkpl<R>(t.gmfp1[o], t.gmfp0[o]);
             b.cohe = mkpl<R>(t.cohe1[o], t.cohe0[o]);
             b.gbr1 = mkpl<R>(t.gbr11[o], t.gbr10[o]);
             b.gbr2 = mkpl<R>(t.gbr21[o], t.gbr20[o]);
-            pmax[o] = mkpl<R>(t.pmax1[o], t.pmax0[o]);
+            L.pmax[o] = mkpl<R>(t.pmax1[o], t.pmax0[o]);
         }
         for (int j = 0; j < D_MXRAYFF; j++) {
             size_t o = (size_t)im * D_MXRAYFF + j;
-            ray[im].xgrid[j] = t.xgrid[o];
-            ray[im].fcum[j] = t.fcum[o];
-            ray[im].b[j] = t.b_array[o];
-            ray[im].c[j] = t.c_array[o];
-            ray[im].ia[j] = t.i_array[o];
+            L.ray[im].xgrid[j] = t.xgrid[o];
+            L.ray[im].fcum[j] = t.fcum[o];
+            L.ray[im].b[j] = t.b_array[o];
+            L.ray[im].c[j] = t.c_array[o];
+            L.ray[im].ia[j] = t.i_array[o];
         }
         for (int q = 0; q < 2; q++)
             for (int j = 0; j < D_MXEKE; j++) {
                 size_t o = (size_t)im * D_MXEKE + j;
-                ElBin<R> &b = el[((size_t)im * 2 + q) * D_MXEKE + j];
+                ElBin<R> &b = L.el[((size_t)im * 2 + q) * D_MXEKE + j];
                 if (q == 0) {
                     b.sig = mkpl<R>(t.esig1[o], t.esig0[o]);
                     b.dedx = mkpl<R>(t.ededx1[o], t.ededx0[o]);
@@ -152,27 +147,57 @@ static int build_devset(omc_engine *e, DevSet<R> &S) {
                 b.earr = (R)t.e_array[o];
             }
     }
-    std::vector<MsE<R>> msurf(D_NMS);
+    L.msurf.assign(D_NMS, MsE<R>{});
     for (int i = 0; i < D_NMS; i++) {
-        msurf[i].u = (R)t.ums[i];
-        msurf[i].f = (R)t.fms[i];
-        msurf[i].w = (R)t.wms[i];
-        msurf[i].i = t.ims[i];
+        L.msurf[i].u = (R)t.ums[i];
+        L.msurf[i].f = (R)t.fms[i];
+        L.msurf[i].w = (R)t.wms[i];
+        L.msurf[i].i = t.ims[i];
     }
-    if ((rc = upload(e, S.ms, ms))) return rc;
-    if ((rc = upload(e, S.ph, phb))) return rc;
-    if ((rc = upload(e, S.pmax, pmax))) return rc;
-    if ((rc = upload(e, S.ray, ray))) return rc;
-    if ((rc = upload(e, S.el, el))) return rc;
-    if ((rc = upload(e, S.msurf, msurf))) return rc;
-    if ((rc = upload(e, S.spin, cvt(t.spin_rej)))) return rc;
+    L.spin.assign(t.spin_rej.begin(), t.spin_rej.end());
+    d.b2spin_min = t.b2spin_min; d.dbeta2i = t.dbeta2i; d.espml = t.espml; d.dleneri = t.dleneri;
+    d.dqq1i = t.dqq1i; d.dllambi = t.dllambi; d.dqmsi = t.dqmsi;
+}
+template void make_layout<double>(const Tables &, const Phantom &, const Regions &, double, double, int,
+                                  Layout<double> &);
+template void make_layout<float>(const Tables &, const Phantom &, const Regions &, double, double, int,
+                                 Layout<float> &);
+
+template <typename R>
+void point_layout_at_host(Layout<R> &L) {
+    DevData<R> &d = L.d;
+    d.xb = L.xb.data(); d.yb = L.yb.data(); d.zb = L.zb.data();
+    d.med = L.med.data(); d.rhof = L.rhof.data();
+    d.ms = L.ms.data(); d.ph = L.ph.data(); d.pmax = L.pmax.data(); d.ray = L.ray.data(); d.el = L.el.data();
+    d.msurf = L.msurf.data(); d.spin = L.spin.data();
+}
+template void point_layout_at_host<double>(Layout<double> &);
+template void point_layout_at_host<float>(Layout<float> &);
+
+template <typename R>
+static int build_devset(omc_engine *e, DevSet<R> &S) {
+    Layout<R> L;
+    make_layout<R>(e->tabs, e->ph, e->reg, e->opt.ecut, e->opt.pcut, e->opt.ref_compat, L);
+    int rc;
+    if ((rc = upload(e, S.xb, L.xb))) return rc;
+    if ((rc = upload(e, S.yb, L.yb))) return rc;
+    if ((rc = upload(e, S.zb, L.zb))) return rc;
+    if ((rc = upload(e, S.med, L.med))) return rc;
+    if ((rc = upload(e, S.rhof, L.rhof))) return rc;
+    if ((rc = upload(e, S.ms, L.ms))) return rc;
+    if ((rc = upload(e, S.ph, L.ph))) return rc;
+    if ((rc = upload(e, S.pmax, L.pmax))) return rc;
+    if ((rc = upload(e, S.ray, L.ray))) return rc;
+    if ((rc = upload(e, S.el, L.el))) return rc;
+    if ((rc = upload(e, S.msurf, L.msurf))) return rc;
+    if ((rc = upload(e, S.spin, L.spin))) return rc;
+    S.d = L.d;
+    DevData<R> &d = S.d;
     d.xb = S.xb.template as<R>(); d.yb = S.yb.template as<R>(); d.zb = S.zb.template as<R>();
     d.med = S.med.template as<int8_t>(); d.rhof = S.rhof.template as<R>();
     d.ms = S.ms.template as<MedS<R>>(); d.ph = S.ph.template as<PhBin<R>>(); d.pmax = S.pmax.template as<PL<R>>();
-    d.ray = S.ray.template as<Rayl<R>>(); d.el = S.el.template as<ElBin<R>>(); d.msurf = S.msurf.template as<MsE<R>>();
-    d.spin = S.spin.template as<R>();
-    d.b2spin_min = t.b2spin_min; d.dbeta2i = t.dbeta2i; d.espml = t.espml; d.dleneri = t.dleneri;
-    d.dqq1i = t.dqq1i; d.dllambi = t.dllambi; d.dqmsi = t.dqmsi;
+    d.ray = S.ray.template as<Rayl<R>>(); d.el = S.el.template as<ElBin<R>>();
+    d.msurf = S.msurf.template as<MsE<R>>(); d.spin = S.spin.template as<R>();
     return OMC_OK;
 }
 

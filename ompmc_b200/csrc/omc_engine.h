@@ -37,6 +37,25 @@ struct DevSet {
     DevData<R> d{};
 };
 
+// Host image of the device layout (built once, then uploaded).
+template <typename R>
+struct Layout {
+    std::vector<R> xb, yb, zb, rhof, spin;
+    std::vector<int8_t> med;
+    std::vector<MedS<R>> ms;
+    std::vector<PhBin<R>> ph;
+    std::vector<PL<R>> pmax;
+    std::vector<Rayl<R>> ray;
+    std::vector<ElBin<R>> el;
+    std::vector<MsE<R>> msurf;
+    DevData<R> d{};
+};
+template <typename R>
+void make_layout(const Tables &t, const Phantom &ph, const Regions &rg, double ecut, double pcut, int ref_compat,
+                 Layout<R> &L);
+template <typename R>
+void point_layout_at_host(Layout<R> &L);
+
 struct KernelStats {
     double seconds = 0;     // device time of the transport kernels
     long launches = 0;      // kernel launches in the transport

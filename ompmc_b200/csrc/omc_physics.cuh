@@ -10,7 +10,9 @@
 // Templates:
 //   R    float (event-based FP32 transport) or double (plain FP64 form)
 //   Env  the environment: R uni(); void deposit(int ir, R e);
-//        bool push(const Part<R>&); void err(unsigned)
+//        bool push(const Part<R>&); void err(unsigned); bool tick() (false
+//        once the history's transport-step budget is spent; every loop
+//        that could run away is bounded by it or by a local guard)
 //
 // Reference quirks reproduced when D.ref_compat != 0 (the default) are
 // marked "quirk"; each is listed in the design notes.
@@ -144,6 +146,7 @@ OMC_HD R hownear(const DevData<R> &D, const Part<R> &p) {
 template <typename R, typename Env>
 OMC_HD void azimuth(Env &g, R &cphi, R &sphi) {
     R x, x2, y, y2, r2;
+    int guard = 0;
     do {
         x = g.uni();
         x = R(2) * x - R(1);
@@ -151,6 +154,7 @@ OMC_HD void azimuth(Env &g, R &cphi, R &sphi) {
         y = g.uni();
         y2 = y * y;
         r2 = x2 + y2;
+        if (++guard > 1000) { g.err(ERR_LOOP); x2 = R(1); y2 = R(0); x = R(1); y = R(0); r2 = R(1); break; }
     } while (r2 > R(1));
     r2 = R(1) / r2;
     cphi = (x2 - y2) * r2;
@@ -205,13 +209,15 @@ OMC_HD Part<R> uphi32(const Part<R> &p, const Uphi<R> &h, R costhe, R sinthe) {
 template <typename R, typename Env>
 OMC_HD void rayleigh(const DevData<R> &D, Env &g, Part<R> &p, int imed, R gle, int lgle) {
     R eig = p.e;
-    R pmax = pwl(D.pmax[imed * D_MXGE + (lgle < 0 ? 0 : lgle)], gle);
+    R pmax = pwl(D.pmax[imed * D_MXGE + (lgle < 0 ? 0 : (lgle > D_MXGE - 1 ? D_MXGE - 1 : lgle))], gle);
     R xmax = R(80.65506856998) * eig;
     const Rayl<R> &ry = D.ray[D.ref_compat ? 0 : imed];
     R rnno0, rnno1, xv, costhe, csqthe;
+    int guard = 0;
     do {
         rnno1 = g.uni();
         do {
+            if (++guard > 100000) { g.err(ERR_LOOP); xv = R(0); break; }
             rnno0 = g.uni();
             rnno0 *= pmax;
             int ibin = D.ref_compat ? 0 : (int)(rnno0 * R(99));
@@ -514,7 +520,7 @@ OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
             imed = D.med[irl];
         }
         if (imed != -1 && dpmfp <= R(1.0E-5)) break;
-        if (++guard > 1000000) { g.err(ERR_LOOP); return false; }
+        if (++guard > 100000 || !g.tick()) { g.err(ERR_LOOP); return false; }
     }
     rnno = g.uni();
     if (rnno <= R(1) - cohfac) {
@@ -1209,7 +1215,12 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
             }
         }
         do {  // ustep loop
-            if (++guard > 200000) { g.err(ERR_LOOP); return E_DEAD; }
+            if (++guard > 20000 || !g.tick()) { g.err(ERR_LOOP); return E_DEAD; }
+            // quirk: the reference declares total_tstep inside this loop
+            // (ompmc.c:4799), so every step after the first of a tstep cycle
+            // sees tstep = 0, takes a zero-length single-scattering step
+            // (one draw) and restarts the cycle with a new demfp.
+            if (D.ref_compat) total_tstep = R(0);
             bool call_howfar, do_single = false, called_msdist = false;
             R tstep, tustep, de = 0, tvstep = 0, range = 0;
             R xf = 0, yf = 0, zf = 0, uf = 0, vf = 0, wf = 0;

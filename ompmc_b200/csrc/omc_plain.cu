@@ -13,6 +13,9 @@
 namespace omc {
 
 constexpr int PLAIN_STACK = 48;
+// Transport steps (photon voxel steps + electron CH steps) one history may
+// take before it is stopped with ERR_LOOP; typical histories take < 1e3.
+constexpr long HISTORY_BUDGET = 2000000;
 
 template <typename Rng>
 struct PlainEnv {
@@ -22,6 +25,8 @@ struct PlainEnv {
     int top;             // slot of the particle being processed
     int nchild;          // particles pushed above it
     unsigned flags;
+    long work;
+    __device__ bool tick() { return ++work < HISTORY_BUDGET; }
     __device__ double uni() { return rng.uni(); }
     __device__ void deposit(int ir, double e) {
         if (ir > 0 && e != 0.0) atomicAdd(&endep[ir - 1], e);
@@ -44,6 +49,7 @@ template <typename Env>
 __device__ void shower(const DevData<double> &D, Env &g, Part<double> *st) {
     int np = 0;
     long steps = 0;
+    g.work = 0;
     while (np >= 0) {
         Part<double> p = st[np];
         g.top = np;
@@ -56,11 +62,11 @@ __device__ void shower(const DevData<double> &D, Env &g, Part<double> *st) {
             for (int k = 0; k < g.nchild; k++) st[np + k] = st[np + 1 + k];
             np += g.nchild - 1;
         }
-        if (++steps > 10000000) {
+        if (++steps > 100000) {
             g.err(ERR_LOOP);
             break;
         }
-        if (g.flags & ERR_RNG) break;
+        if (g.flags & (ERR_RNG | ERR_LOOP)) break;
     }
 }
 
@@ -156,6 +162,8 @@ struct ReplayEnv {
     int *dep_ir;
     double *dep_e;
     int dep_cap, ndep;
+    long work;
+    __device__ bool tick() { return ++work < HISTORY_BUDGET; }
     __device__ double uni() { return rng.uni(); }
     __device__ void deposit(int ir, double e) {
         if (ndep < dep_cap) {

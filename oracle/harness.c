@@ -25,6 +25,8 @@
  *                               deposit sequences per history
  *   h_replay(...)               run one history on a scripted stream
  */
+#define _GNU_SOURCE
+#include <dlfcn.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -57,7 +59,16 @@ static double *rn_buf = NULL;     /* record target or replay source */
 static long rn_cap = 0, rn_pos = 0;
 static int rn_overflow = 0;
 
+/* Optional draw log: the function that called setRandom for each draw. */
+static const char **draw_site = NULL;
+static long draw_cap = 0;
+
 double setRandom(void) {
+    if (draw_site && rn_pos < draw_cap) {
+        Dl_info info;
+        void *ra = __builtin_return_address(0);
+        draw_site[rn_pos] = (dladdr(ra, &info) && info.dli_sname) ? info.dli_sname : "?";
+    }
     if (rng_mode == 2) {
         if (rn_pos < rn_cap) return rn_buf[rn_pos++];
         rn_overflow = 1;
@@ -77,12 +88,14 @@ static int *dep_ir = NULL;
 static double *dep_e = NULL;
 static long dep_cap = 0, dep_pos = 0;
 static int dep_overflow = 0;
+static long *dep_rnpos = NULL;   /* optional: random numbers drawn before each deposit */
 
 void ausgab(double edep) {
     if (dep_log_on) {
         if (dep_pos < dep_cap) {
             dep_ir[dep_pos] = stack.ir[stack.np];
             dep_e[dep_pos] = stack.wt[stack.np] * edep;
+            if (dep_rnpos) dep_rnpos[dep_pos] = rn_pos;
         } else {
             dep_overflow = 1;
         }
@@ -282,6 +295,20 @@ long h_replay(const double *q, const double *rn, long n, int *dir, double *de,
     dep_log_on = 0;
     *ndep = dep_pos;
     return (rn_overflow || dep_overflow) ? -1 : rn_pos;
+}
+
+void h_trace_draws(const char **sites, long cap) {
+    draw_site = sites;
+    draw_cap = cap;
+}
+
+/* h_replay with the count of random numbers drawn before each deposit. */
+long h_replay_traced(const double *q, const double *rn, long n, int *dir, double *de, long *rnpos,
+                     long d_capacity, long *ndep) {
+    dep_rnpos = rnpos;
+    long r = h_replay(q, rn, n, dir, de, d_capacity, ndep);
+    dep_rnpos = NULL;
+    return r;
 }
 
 /* Sampler entry points on a hand-set stack top with a scripted stream.
