@@ -64,7 +64,12 @@ struct KernelStats {
 
 }  // namespace omc
 
+namespace omc {
+struct EventState;
+}
+
 struct omc_engine {
+    omc::EventState *ev = nullptr;  // event-form queues (allocated on first use)
     omc::Tables tabs;
     omc::Phantom ph;
     omc::Regions reg;

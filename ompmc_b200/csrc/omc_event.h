@@ -3,6 +3,43 @@
 #include "omc_engine.h"
 
 namespace omc {
+
+// Structure-of-arrays particle queue in device memory.  `tag` packs the
+// charge (iq+1, 2 bits) and the tally slot (upper bits); k0/k1 are the
+// particle's Philox stream key and ctr its block counter.
+struct Queue {
+    float *x, *y, *z, *u, *v, *w, *e, *wt;
+    int *ir, *tag;
+    uint32_t *k0, *k1, *ctr;
+    int *count;      // device counter of occupied entries
+    int cap;
+};
+
+// Cycle control block in device memory.
+struct Ctl {
+    int cnt[4];               // photon A, electron A, photon B, electron B
+    long long hist_next;      // next history to inject
+    long long hist_total;     // histories requested
+    int inject;               // histories injected this cycle
+    int inject_base_lo;       // unused padding
+    long long hist_base;      // first history of this cycle's injection
+    unsigned flags;           // DevErr bits
+    int pad;
+    double src_energy;        // sum of primary kinetic energies
+    double edep;              // unused
+};
+
+struct EventState {
+    bool ready = false;
+    int cap = 0;              // per queue
+    DBuf buf[4];              // photon A, electron A, photon B, electron B (13 arrays each)
+    Queue q[4];
+    DBuf ctl;
+    Ctl *ctl_d = nullptr;
+    int block = 256;
+    int grid = 0;
+};
+
 int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint64_t seed, double *sum, double *sum2,
                    double *src_energy, KernelStats &ks);
 void event_release(omc_engine *e);
