@@ -1,0 +1,358 @@
+"""Benchmark: histories/s of the event-based FP32-transport / FP64-tally form
+on the heterogeneous slab workload (64^3 voxels of 0.25 cm: water 0-3 cm,
+lung 3-8 cm, bone 8-10 cm, water; 5x5 cm^2 field of the 6 MV-like spectrum,
+10^7 histories = 10 steps of 10^6), one JSON line on stdout.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one complete dose run of 10^6 histories in 10 batches through
+omc_run_beam (dose + batch uncertainty out).  `value` is device time of the
+transport (CUDA events on the engine's stream, tables/phantom resident);
+`e2e` times the same calls from the host with the spectrum upload and the
+dose/uncertainty download inside.  Under torchrun every rank runs its own
+histories on its own GPU (weak scaling, no collective on the data path); the
+reported time is the maximum over ranks.
+
+`--impl reference` times ompMC's own OpenMP CLI (built from its sources into
+oracle/_ref) on this host's cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "histories/s at 1% dose unc. (served vs plain GPU vs CPU); p50/p99 beamlet ms"
+WORKLOAD = "slab64: 64^3 x 0.25 cm water/lung(0.26)/bone(1.85)/water, 5x5 cm2 6MV-like, 1e6 histories x 10 batches per step"
+HIST_PER_STEP = 1_000_000
+NBATCH = 10
+COLLIMATOR = (-2.5, 2.5, -2.5, 2.5)
+MEDIA = ["H2O521ICRU", "LUNG521ICRU", "ICRPBONE521ICRU"]
+
+
+def peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def workload_inputs():
+    from ompmc_b200 import assets as A
+    root = A.require_assets()
+    ph = A.slab_phantom(64, 0.25)
+    spec_path = root / "spectra" / "6mv.spectrum"
+    if not spec_path.exists():
+        A.write_spectrum(spec_path, "6mv")
+    return root, ph, spec_path
+
+
+def mean_unc_above_half(dose, unc):
+    m = dose > 0.5 * dose.max()
+    return float(unc[m].mean())
+
+
+def atomic_peak(device, n_vox):
+    """Measured FP64 scattered-add throughput (torch index_add_ on the GPU):
+    the denominator for the tally-atomic fraction."""
+    import torch
+    dev = torch.device("cuda", device)
+    tally = torch.zeros(n_vox, dtype=torch.float64, device=dev)
+    n = 1 << 24
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    idx = torch.randint(0, n_vox, (n,), device=dev, generator=g)
+    val = torch.rand(n, dtype=torch.float64, device=dev, generator=g)
+    for _ in range(3):
+        tally.index_add_(0, idx, val)
+    torch.cuda.synchronize(dev)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    reps = 10
+    for _ in range(reps):
+        tally.index_add_(0, idx, val)
+    e.record()
+    torch.cuda.synchronize(dev)
+    return n * reps / (s.elapsed_time(e) * 1e-3)
+
+
+def ncu_traffic_per_event():
+    """DRAM bytes per electron event from the committed ncu summary."""
+    p = REPO / "profiles" / "electron_transport_slab64.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("dram_bytes_per_event:"):
+            try:
+                return float(line.split(":")[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def reference_rate(root, ph, spec_path, ncase, cores):
+    """ompMC CLI (oracle/_ref) on `cores` host cores; histories/s of its batch loop."""
+    from oracle import ref
+    from ompmc_b200 import assets as A
+    work = root / "bench"
+    work.mkdir(parents=True, exist_ok=True)
+    pf = work / "slab64.egsphant"
+    if not pf.exists():
+        A.write_egsphant(pf, ph)
+    run = A.default_run(pf, ncase=ncase, nbatch=NBATCH, collimator=COLLIMATOR, output_folder=str(work) + "/")
+    base = work / f"ref_{ncase}"
+    A.write_inp(base, run)
+    loop_s, _ = ref.run_cli(base, f"ref_{ncase}", cores=cores)
+    return ncase / loop_s, loop_s
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs an ompMC checkout at build time)"}))
+        return 0
+    root, ph, spec = workload_inputs()
+    cores = host_cores()
+    sample = args.ref_sample
+    for _ in range(args.warmup):
+        reference_rate(root, ph, spec, sample // 4, cores)
+    rates, secs = [], []
+    for _ in range(args.steps):
+        r, s = reference_rate(root, ph, spec, sample, cores)
+        rates.append(r)
+        secs.append(s)
+    total = sample * args.steps
+    value = total / sum(secs)
+    out = {
+        "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * sum(secs) / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "sample_histories_per_step": sample, "parallelism": f"openmp{cores}"},
+        "cpu_baseline": {"value": value, "unit": "histories/s", "cores": cores, "kind": "reference",
+                         "sample": f"{sample} histories x {args.steps} runs of the ompMC CLI (slab64)"},
+        "e2e": {"value": value, "unit": "histories/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="event", choices=["event", "plain"])
+    ap.add_argument("--hist-per-step", type=int, default=HIST_PER_STEP)
+    ap.add_argument("--ref-sample", type=int, default=400_000)
+    ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and plain comparator")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from ompmc_b200.engine import EVENT_FP32, PLAIN_FP64, Engine, Tables, load_spectrum
+    root, ph, spec_path = workload_inputs()
+    spec = load_spectrum(spec_path)
+    tables = Tables.from_assets(MEDIA, root)
+    eng = Engine(tables, ph, ecut=0.7, pcut=0.01, device=local)
+    mode = EVENT_FP32 if args.mode == "event" else PLAIN_FP64
+    nstep = args.hist_per_step
+    seed0 = 1000003 * (rank + 1)
+
+    def step(i, e=eng, m=mode, n=nstep):
+        return e.run_beam(n, NBATCH, seed=seed0 + i, mode=m, spectrum=spec, collimator=COLLIMATOR)
+
+    for i in range(args.warmup):
+        step(-1 - i)
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    t0 = time.perf_counter()
+    dev_s = 0.0
+    launches = 0
+    uncs = []
+    for i in range(args.steps):
+        dose, unc, st = step(i)
+        dev_s += st["seconds"]
+        launches += st["launches"]
+        uncs.append(mean_unc_above_half(dose, unc))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    if dist:
+        t = torch.tensor([dev_s, wall], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s, wall = float(t[0]), float(t[1])
+    total = nstep * args.steps * world
+    value = total / dev_s
+    e2e = total / wall
+    nvox = int(np.prod(eng.shape))
+
+    extras = {}
+    if rank == 0:
+        # roofline of the dominant kernel from a profiled (untimed) step
+        peak, peak_kind = peaks()
+        prof_eng = Engine(tables, ph, ecut=0.7, pcut=0.01, device=local, profile=True)
+        prof_eng.run_beam(nstep, NBATCH, seed=777, mode=EVENT_FP32, spectrum=spec, collimator=COLLIMATOR)
+        prof = prof_eng.profile_last()
+        prof_eng.close()
+        ek = prof["electron"]
+        pk = prof["photon"]
+        lookups = 10 * ek["steps"] + 3 * ek["particles"]
+        alg_bytes = 8 * ek["cross"] + 16 * ek["dep"] + 8 * lookups
+        achieved = alg_bytes / ek["seconds"] / 1e9
+        tpe = ncu_traffic_per_event()
+        per_launch_events = ek["particles"] / max(1, ek["launches"])
+        extras["roofline"] = {
+            "bound": "hbm", "kernel": "k_electron_step", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": (tpe * per_launch_events) if tpe else None,
+            "algorithmic_bytes_per_launch": alg_bytes / max(1, ek["launches"]),
+            "avg_launch_ms": 1000 * ek["seconds"] / max(1, ek["launches"]),
+            "kernel_share": {k: v["seconds"] for k, v in prof.items()},
+        }
+        hist = nstep
+        per_hist = {k: ek[k] / hist + pk[k] / hist for k in ("particles", "steps", "cross", "dep", "atom")}
+        try:
+            apk = atomic_peak(local, nvox)
+            atom_rate = (ek["atom"] + pk["atom"]) / (ek["seconds"] + pk["seconds"])
+            extras["atomics"] = {"tally_atomics_per_s_in_kernels": atom_rate, "measured_fp64_scatter_peak": apk,
+                                 "frac": atom_rate / apk}
+        except Exception as ex:  # the torch microbenchmark is optional
+            extras["atomics"] = {"error": str(ex)[:200]}
+        extras["per_history"] = per_hist
+        unc1 = float(np.mean(uncs))
+        extras["dose_unc"] = {"mean_rel_unc_gt50pct_dmax": unc1, "histories_per_step": nstep,
+                              "histories_to_1pct": nstep * (unc1 / 0.01) ** 2,
+                              "seconds_to_1pct": nstep * (unc1 / 0.01) ** 2 / value}
+        if not args.no_extras and world == 1:
+            # plain FP64 history-based form on the same workload (comparator)
+            pn = max(nstep // 2, 100000)
+            step(999, m=PLAIN_FP64, n=pn)
+            _, _, pst = step(1000, m=PLAIN_FP64, n=pn)
+            plain = pn / pst["seconds"]
+            extras["plain_fp64"] = {"value": plain, "unit": "histories/s", "speedup_event_vs_plain": value / plain}
+            # CPU reference on this host's cores (bounded sample)
+            from oracle import ref
+            if ref.available():
+                cores = host_cores()
+                r, s = reference_rate(root, ph, spec_path, args.ref_sample, cores)
+                extras["cpu_baseline"] = {"value": r, "unit": "histories/s", "cores": cores, "kind": "reference",
+                                          "sample": f"{args.ref_sample} histories of the slab64 workload, ompMC CLI, "
+                                                    f"{s:.1f} s batch loop"}
+            else:
+                extras["cpu_baseline"] = None
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if mode == EVENT_FP32 else "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "mode": args.mode, "histories_per_step_per_gpu": nstep,
+                       "tally": "f64", "parallelism": f"replicas{world}",
+                       "l2": "particle queues (0.8 GB) and batch tallies exceed L2; physics tables are L2-resident"},
+            "e2e": {"value": e2e, "unit": "histories/s", "h2d_bytes_per_step": 2 * 1000 * 8 + 64,
+                    "d2h_bytes_per_step": 2 * nvox * 8},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        out.update(extras)
+        print(json.dumps(out))
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -79,6 +79,11 @@ typedef struct {
     int64_t queue_capacity; /* event form: particles per queue (0 = default) */
     int block;            /* threads per block (0 = default) */
     int nsplit;           /* photon splitting: only 1 is supported */
+    int profile;          /* 1: event form launches cycles one by one and times
+                             every kernel (see omc_profile_last) */
+    int electron_tsteps;  /* event form: tstep-loop iterations an electron runs
+                             per launch before it is re-queued (0 = default) */
+    int64_t inflight;     /* event form: particles kept in flight (0 = default) */
 } omc_options;
 
 void omc_options_default(omc_options *o);
@@ -88,6 +93,15 @@ typedef struct omc_engine omc_engine;
 int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_options *o, omc_engine **out);
 int omc_engine_destroy(omc_engine *e);
 const char *omc_engine_last_error(const omc_engine *e);
+
+/* Per-kernel profile of the last event-form omc_run_beam made with
+ * options.profile = 1.  out (n >= 28) receives, for kernel k = 0 source,
+ * 1 photon transport, 2 electron transport, 3 plan + reset, the values
+ * out[k*7 + j]: j = 0 launches, 1 device seconds, 2 particles processed,
+ * 3 transport steps (photon voxel steps, electron CH/BCA steps),
+ * 4 voxel-boundary crossings, 5 energy deposits, 6 FP64 tally atomics
+ * (deposits into one voxel in a row are summed first). */
+int omc_profile_last(const omc_engine *e, double *out, int n);
 
 /* ------------------------------------------------------------ sources */
 /* Energy distribution: a spectrum inverse CDF (cdf1/cdf2 of length n,

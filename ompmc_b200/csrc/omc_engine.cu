@@ -544,6 +544,18 @@ int omc_engine_destroy(omc_engine *e) {
 
 const char *omc_engine_last_error(const omc_engine *e) { return e ? e->err.c_str() : omc_last_error(); }
 
+int omc_profile_last(const omc_engine *e, double *out, int n) {
+    if (!e || !out || n < 28) return global_err(OMC_E_ARG, "omc_profile_last: bad argument");
+    for (int i = 0; i < 28; i++) out[i] = 0;
+    if (!e->ev) return OMC_OK;
+    for (int k = 0; k < 4; k++) {
+        const KernelProfile &P = e->ev->prof[k];
+        double v[7] = {P.launches, P.seconds, P.particles, P.steps, P.cross, P.dep, P.atom};
+        for (int j = 0; j < 7; j++) out[k * 7 + j] = v[j];
+    }
+    return OMC_OK;
+}
+
 // ------------------------------------------------------------ beam runs
 int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, uint64_t seed, int mode, double *dose,
                  double *unc, double *stats) {

@@ -40,9 +40,11 @@ struct EvEnv {
     int nout;
     unsigned flags;
     int work;
+    int ncross, ndep, natom;
     __device__ float uni() { return rng.uni(); }
     // Consecutive deposits into one voxel are summed before the atomic.
     __device__ void deposit(int ir, float e) {
+        ndep++;
         if (ir != pend_ir) {
             flush();
             pend_ir = ir;
@@ -50,10 +52,16 @@ struct EvEnv {
         pend_e += (double)e;
     }
     __device__ void flush() {
-        if (pend_ir > 0 && pend_e != 0.0) atomicAdd(&tally[pend_ir - 1], pend_e);
+        if (pend_ir > 0 && pend_e != 0.0) {
+            atomicAdd(&tally[pend_ir - 1], pend_e);
+            natom++;
+        }
         pend_e = 0.0;
         pend_ir = -1;
     }
+    __device__ void cross() { ncross++; }
+    int tsteps;
+    __device__ int tstep_budget() const { return tsteps; }
     __device__ bool push(const Part<float> &q) {
         if (nout >= EV_MAXOUT) {
             flags |= ERR_STACK;
@@ -164,11 +172,18 @@ __device__ __forceinline__ void report_flags(Ctl *ctl, unsigned flags, unsigned 
     if (f && (threadIdx.x & 31) == __ffs(active) - 1) atomicOr(&ctl->flags, f);
 }
 
+__device__ __forceinline__ void report_count(unsigned long long *dst, unsigned v, unsigned active) {
+    unsigned t = __reduce_add_sync(active, v);
+    if (t && (threadIdx.x & 31) == __ffs(active) - 1) atomicAdd(dst, (unsigned long long)t);
+}
+
 template <bool PHOTON>
-__global__ void __launch_bounds__(256) k_transport(DevData<float> D, Queue in, Queue outP, Queue outE,
-                                                   double *tallies, long nvox, Ctl *ctl, uint32_t seedw) {
+__device__ __forceinline__ void transport_events(const DevData<float> &D, const Queue &in, const Queue &outP,
+                                                 const Queue &outE, double *tallies, long nvox, Ctl *ctl,
+                                                 uint32_t seedw, int tsteps) {
     int n = min(*in.count, in.cap);
     unsigned flags = 0;
+    unsigned c_ev = 0, c_steps = 0, c_cross = 0, c_dep = 0, c_atom = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         unsigned active = __activemask();
         Part<float> p;
@@ -184,15 +199,43 @@ __global__ void __launch_bounds__(256) k_transport(DevData<float> D, Queue in, Q
         g.nout = 0;
         g.flags = 0;
         g.work = 0;
+        g.tsteps = tsteps;
+        g.ncross = g.ndep = g.natom = 0;
         bool alive;
         if (PHOTON) alive = photon_step(D, g, p);
         else alive = electron_step(D, g, p) == E_ALIVE;
         g.flush();
         emit(outP, outE, active, alive, p, g, slot, k0, k1);
         flags |= g.flags;
+        c_ev++;
+        c_steps += g.work;
+        c_cross += g.ncross;
+        c_dep += g.ndep;
+        c_atom += g.natom;
     }
     unsigned active = __activemask();
     report_flags(ctl, flags, active);
+    const int k = PHOTON ? 0 : 1;
+    report_count(&ctl->st_events[k], c_ev, active);
+    report_count(&ctl->st_steps[k], c_steps, active);
+    report_count(&ctl->st_cross[k], c_cross, active);
+    report_count(&ctl->st_dep[k], c_dep, active);
+    report_count(&ctl->st_atom[k], c_atom, active);
+}
+
+// One photon event per queued photon.
+__global__ void __launch_bounds__(256) k_photon_step(DevData<float> D, Queue in, Queue outP, Queue outE,
+                                                     double *tallies, long nvox, Ctl *ctl, uint32_t seedw) {
+    transport_events<true>(D, in, outP, outE, tallies, nvox, ctl, seedw, 1 << 30);
+}
+
+// One bounded electron/positron event per queued charged particle: at most
+// `tsteps` iterations of electron()'s tstep loop, then the particle is
+// re-queued, so every lane of a warp does a similar amount of work.
+__global__ void __launch_bounds__(256) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
+                                                       double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
+                                                       int tsteps) {
+    transport_events<false>(D, in, outP, outE, tallies, nvox, ctl, seedw, tsteps);
 }
 
 __global__ void k_source(DevData<float> D, BeamSrc<float> S, Queue qP, Queue qE, Ctl *ctl, long long nper,
@@ -267,6 +310,9 @@ static int event_prepare(omc_engine *e) {
     S.cap = (int)std::min(cap, (long)(1L << 30));
     S.block = e->opt.block > 0 ? e->opt.block : 256;
     S.grid = e->sm_count * (2048 / S.block);
+    // 2 measured best on the slab workload (sweep of 1..16 on a B200)
+    S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 2;
+    S.inflight = e->opt.inflight > 0 ? e->opt.inflight : (1LL << 20);
     int rc = S.ctl.alloc(sizeof(Ctl));
     if (rc) return set_err(e, rc, "control block allocation failed");
     S.ctl_d = S.ctl.as<Ctl>();
@@ -281,21 +327,66 @@ void event_release(omc_engine *e) {
     e->ev = nullptr;
 }
 
-// One transport cycle with input buffers `in` (0 = A, 1 = B).
+// One transport cycle with input buffers `in` (0 = A, 1 = B).  With `ev`
+// (profiling) an event is recorded before each launch and after the last.
 static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, double *tallies, long nper, uint64_t seed,
-                         long long target) {
+                         long long target, cudaEvent_t *ev = nullptr) {
     EventState &S = *e->ev;
     int iph = in == 0 ? 0 : 2, iel = iph + 1;
     int oph = in == 0 ? 2 : 0, oel = oph + 1;
     uint32_t seedw = (uint32_t)(seed >> 32);
     long nvox = e->ph.nvox();
+    if (ev) cudaEventRecord(ev[0], e->stream);
     k_plan<<<1, 1, 0, e->stream>>>(S.ctl_d, iph, iel, target, S.cap);
+    if (ev) cudaEventRecord(ev[1], e->stream);
     k_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, src, S.q[iph], S.q[iel], S.ctl_d, nper, seed, seedw);
-    k_transport<true><<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
+    if (ev) cudaEventRecord(ev[2], e->stream);
+    k_photon_step<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
                                                           S.ctl_d, seedw);
-    k_transport<false><<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
-                                                           S.ctl_d, seedw);
+    if (ev) cudaEventRecord(ev[3], e->stream);
+    k_electron_step<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
+                                                           S.ctl_d, seedw, S.tsteps);
+    if (ev) cudaEventRecord(ev[4], e->stream);
     k_reset<<<1, 1, 0, e->stream>>>(S.ctl_d, iph, iel);
+    if (ev) cudaEventRecord(ev[5], e->stream);
+}
+
+// Profiled transport: cycles launched one by one with events around each
+// kernel; per-kernel device time accumulated into S.prof.
+static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallies, long nper, uint64_t seed,
+                        long long target, Ctl &h, long &cycles) {
+    EventState &S = *e->ev;
+    for (auto &p : S.prof) p = KernelProfile();
+    cudaEvent_t ev[6];
+    for (auto &x : ev) cudaEventCreate(&x);
+    int rc = OMC_OK;
+    cycles = 0;
+    for (;;) {
+        launch_cycle(e, (int)(cycles & 1), src, tallies, nper, seed, target, ev);
+        cycles++;
+        if ((rc = cuda_check(e, cudaEventSynchronize(ev[5]), "profiled cycle"))) break;
+        float t[5];
+        for (int k = 0; k < 5; k++) cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]);
+        S.prof[3].seconds += (t[0] + t[4]) * 1e-3;
+        S.prof[3].launches += 2;
+        S.prof[0].seconds += t[1] * 1e-3;
+        S.prof[0].launches += 1;
+        S.prof[1].seconds += t[2] * 1e-3;
+        S.prof[1].launches += 1;
+        S.prof[2].seconds += t[3] * 1e-3;
+        S.prof[2].launches += 1;
+        if ((cycles & 1) == 0) {
+            cudaMemcpy(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
+            if (h.hist_next >= h.hist_total && h.cnt[0] == 0 && h.cnt[1] == 0) break;
+            if (h.flags & ERR_QUEUE) break;
+        }
+        if (cycles > 200000) {
+            rc = set_err(e, OMC_E_DEVICE, "event transport did not drain");
+            break;
+        }
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+    return rc;
 }
 
 int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint64_t seed, double *sum, double *sum2,
@@ -320,7 +411,40 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
     Ctl c0{};
     c0.hist_total = (long long)nper * nbatch;
     cudaMemcpyAsync(S.ctl_d, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, e->stream);
-    long long target = std::min<long long>((long long)S.cap / 2, 1LL << 20);
+    long long target = std::min<long long>((long long)S.cap / 2, S.inflight);
+
+    if (e->opt.profile) {
+        Ctl h{};
+        long cycles = 0;
+        cudaEvent_t t0, t1;
+        cudaEventCreate(&t0);
+        cudaEventCreate(&t1);
+        cudaEventRecord(t0, e->stream);
+        rc = run_profiled(e, src, tal.as<double>(), nper, seed, target, h, cycles);
+        for (int ib = 0; ib < nbatch && rc == OMC_OK; ib++)
+            rc = fold(e, tal.as<double>() + (size_t)ib * nvox, sum, sum2, nvox, 1.0);
+        cudaEventRecord(t1, e->stream);
+        cudaEventSynchronize(t1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, t0, t1);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        ks.seconds = ms * 1e-3;
+        ks.launches = cycles * 5 + nbatch;
+        ks.flags |= h.flags;
+        for (int k = 0; k < 2; k++) {
+            KernelProfile &P = S.prof[1 + k];
+            P.particles = (double)h.st_events[k];
+            P.steps = (double)h.st_steps[k];
+            P.cross = (double)h.st_cross[k];
+            P.dep = (double)h.st_dep[k];
+            P.atom = (double)h.st_atom[k];
+        }
+        S.prof[0].particles = (double)h.hist_total;
+        if (rc) return rc;
+        cudaMemcpyAsync(src_energy, &S.ctl_d->src_energy, 8, cudaMemcpyDeviceToDevice, e->stream);
+        return OMC_OK;
+    }
 
     // capture two cycles (A -> B, B -> A) as one graph
     cudaGraph_t graph = nullptr;

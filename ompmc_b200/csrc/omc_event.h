@@ -27,6 +27,13 @@ struct Ctl {
     int pad;
     double src_energy;        // sum of primary kinetic energies
     double edep;              // unused
+    // counters per transport kernel (0 photon, 1 electron)
+    unsigned long long st_events[2], st_steps[2], st_cross[2], st_dep[2], st_atom[2];
+};
+
+// Per-kernel profile of the last run made with options.profile = 1.
+struct KernelProfile {
+    double launches = 0, seconds = 0, particles = 0, steps = 0, cross = 0, dep = 0, atom = 0;
 };
 
 struct EventState {
@@ -38,6 +45,9 @@ struct EventState {
     Ctl *ctl_d = nullptr;
     int block = 256;
     int grid = 0;
+    int tsteps = 2;           // electron tstep iterations per event launch
+    long long inflight = 0;   // particles kept in flight by the injector
+    KernelProfile prof[4];    // 0 source, 1 photon, 2 electron, 3 plan+reset
 };
 
 int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint64_t seed, double *sum, double *sum2,

@@ -10,7 +10,10 @@
 // Templates:
 //   R    float (event-based FP32 transport) or double (plain FP64 form)
 //   Env  the environment: R uni(); void deposit(int ir, R e);
-//        bool push(const Part<R>&); void err(unsigned); bool tick() (false
+//        bool push(const Part<R>&); void err(unsigned); void cross() (a
+//        voxel boundary was crossed; counting only); int tstep_budget()
+//        (tstep-loop iterations one electron_step call may run before it
+//        returns the particle unchanged for a later call); bool tick() (false
 //        once the history's transport-step budget is spent; every loop
 //        that could run away is bounded by it or by a local guard)
 //
@@ -518,6 +521,7 @@ OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
             irl = irnew;
             irold = irnew;
             imed = D.med[irl];
+            g.cross();
         }
         if (imed != -1 && dpmfp <= R(1.0E-5)) break;
         if (++guard > 100000 || !g.tick()) { g.err(ERR_LOOP); return false; }
@@ -1195,7 +1199,13 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
     R sig0 = 0, demfp = 0, total_de = 0, total_tstep = 0;
     R ustep = 0;
     int guard = 0;
+    int ntstep = 0;
+    const int tstep_budget = g.tstep_budget();
     for (;;) {  // tstep loop
+        // The top of the tstep loop carries no state but the particle
+        // (demfp is re-drawn here), so an event can stop after a budget of
+        // iterations and resume in a later launch exactly where it was.
+        if (ntstep++ >= tstep_budget) return E_ALIVE;
         bool compute_tstep = true;
         R eke = eie - RMr;
         if (imed != -1) {
@@ -1340,6 +1350,7 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
                     p.ir = irnew;
                     irl = irnew;
                     imed = D.med[irl];
+                    g.cross();
                 }
                 if (eie <= ecut_of(D, irl)) return e_cutoff(D, g, p, eie);
                 break;
@@ -1401,6 +1412,7 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
                 p.ir = irnew;
                 irl = irnew;
                 imed = D.med[irl];
+                g.cross();
             }
             if (eie <= ecut_of(D, irl)) return e_cutoff(D, g, p, eie);
             if (imed != medold) break;

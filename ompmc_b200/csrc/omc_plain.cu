@@ -42,6 +42,8 @@ struct PlainEnv {
         return true;
     }
     __device__ void err(unsigned f) { flags |= f; }
+    __device__ void cross() {}
+    __device__ int tstep_budget() const { return 1 << 30; }
 };
 
 // shower() (ompmc.c:5454-5465) on a local stack.
@@ -185,6 +187,8 @@ struct ReplayEnv {
         return true;
     }
     __device__ void err(unsigned f) { flags |= f; }
+    __device__ void cross() {}
+    __device__ int tstep_budget() const { return 1 << 30; }
 };
 
 __global__ void k_replay(DevData<double> D, const double *prim, int nhist, const double *rn, const long *rn_off,

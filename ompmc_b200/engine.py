@@ -48,7 +48,8 @@ class _Phantom(C.Structure):
 class _Options(C.Structure):
     _fields_ = [("ecut", C.c_double), ("pcut", C.c_double), ("device", C.c_int),
                 ("ref_compat", C.c_int), ("queue_capacity", C.c_int64), ("block", C.c_int),
-                ("nsplit", C.c_int)]
+                ("nsplit", C.c_int), ("profile", C.c_int), ("electron_tsteps", C.c_int),
+                ("inflight", C.c_int64)]
 
 
 class _Energy(C.Structure):
@@ -97,6 +98,7 @@ def lib():
         "omc_run_beamlets": ([C.c_void_p, C.POINTER(_Beamlets), C.c_int64, C.c_int, C.c_double, C.c_uint64, C.c_int,
                               _lp, _ip, _dp, _dp, C.c_int64, _lp, _dp], C.c_int),
         "omc_dosxyz_run": ([C.c_char_p, C.c_char_p, C.c_int, C.c_int], C.c_int),
+        "omc_profile_last": ([C.c_void_p, _dp, C.c_int], C.c_int),
         "omc_trace_rays": ([C.c_void_p, _dp, C.c_int, C.c_int, _dp, _ip, _ip, _ip, _dp], C.c_int),
         "omc_replay": ([C.c_void_p, _dp, C.c_int, _dp, _lp, C.c_int, _ip, _dp, _ip, _lp, _up], C.c_int),
     }
@@ -178,7 +180,7 @@ class Engine:
     """Resident tables + phantom on one GPU."""
 
     def __init__(self, tables: Tables, phantom, ecut=0.7, pcut=0.01, device=0, ref_compat=True,
-                 queue_capacity=0, block=0):
+                 queue_capacity=0, block=0, profile=False, electron_tsteps=0, inflight=0):
         L = lib()
         self.tables = tables
         self.phantom = phantom
@@ -197,6 +199,9 @@ class Engine:
         o.ref_compat = 1 if ref_compat else 0
         o.queue_capacity = queue_capacity
         o.block = block
+        o.profile = 1 if profile else 0
+        o.electron_tsteps = electron_tsteps
+        o.inflight = inflight
         h = C.c_void_p()
         _check(L.omc_engine_create(tables.h, C.byref(P), C.byref(o), C.byref(h)))
         self.h = h
@@ -286,6 +291,14 @@ class Engine:
         b.gaussian = 1 if bl.get("gaussian") else 0
         b.gauss_width = float(bl.get("gauss_width", 0.2123))
         return b
+
+    def profile_last(self):
+        """Per-kernel profile of the last profiled event-form run."""
+        out = np.zeros(28)
+        _check(lib().omc_profile_last(self.h, _p(out, _dp), 28), self.h)
+        names = ["source", "photon", "electron", "plan_reset"]
+        keys = ["launches", "seconds", "particles", "steps", "cross", "dep", "atom"]
+        return {names[k]: dict(zip(keys, out[k * 7:(k + 1) * 7])) for k in range(4)}
 
     # ------------------------------------------------ validation hooks
     def trace_rays(self, rays, cap=512):
