@@ -153,6 +153,29 @@ typedef struct {
 int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, uint64_t seed, int mode,
                  double *dose, double *unc, double *stats);
 
+/* ------------------------------------- fixed-scratch beam run (no alloc)
+ * omc_run_beam in the plain FP64 form for callers that must not allocate
+ * device memory while they run it: cudaMalloc/cudaFree synchronise the
+ * device and take unbounded time, which a latency-bound caller (a plan
+ * optimiser evaluating dose in its loop) cannot afford, and a host whose
+ * GPU memory is owned by its own fixed-budget pool allocator may see an
+ * extra allocation fail.  Create the engine at start-up, then call this.
+ * It has no counterpart in the reference.
+ *
+ * All scratch (batch tallies, sums, outputs before download, spectrum)
+ * lives in one file-scope device array sized for OMC_NOALLOC_MAX_VOXELS
+ * voxels (about 10 MB), held by every GPU that loads the library until the
+ * process exits.  Phantoms above that size are rejected with OMC_E_RANGE.
+ * The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call shares the array and clears it at its start: calls that
+ * overlap on the GPU (other threads, other engines on the same device)
+ * race.  Arguments and results are those of omc_run_beam with mode
+ * OMC_PLAIN_FP64; stats[1] is host wall time of the run. */
+#define OMC_NOALLOC_MAX_VOXELS 262144
+int omc_run_beam_noalloc(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, uint64_t seed, double *dose,
+                         double *unc, double *stats);
+
 /* ------------------------------------------- dose influence (matRad)
  * One sparse column per beamlet, as the matRad MEX entry builds them
  * (omc_matrad.c:1576-1720): per beamlet, nhist histories in nbatch

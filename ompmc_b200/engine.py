@@ -99,6 +99,8 @@ def lib():
                               _lp, _ip, _dp, _dp, C.c_int64, _lp, _dp], C.c_int),
         "omc_dosxyz_run": ([C.c_char_p, C.c_char_p, C.c_int, C.c_int], C.c_int),
         "omc_profile_last": ([C.c_void_p, _dp, C.c_int], C.c_int),
+        "omc_run_beam_noalloc": ([C.c_void_p, C.POINTER(_Beam), C.c_int64, C.c_int, C.c_uint64, _dp, _dp, _dp],
+                                 C.c_int),
         "omc_trace_rays": ([C.c_void_p, _dp, C.c_int, C.c_int, _dp, _ip, _ip, _ip, _dp], C.c_int),
         "omc_replay": ([C.c_void_p, _dp, C.c_int, _dp, _lp, C.c_int, _ip, _dp, _ip, _lp, _up], C.c_int),
     }
@@ -244,6 +246,27 @@ class Engine:
         st = np.zeros(6)
         _check(lib().omc_run_beam(self.h, C.byref(b), int(ncase), int(nbatch), int(seed) & (2**64 - 1), mode,
                                   _p(dose, _dp), _p(unc, _dp), _p(st, _dp)), self.h)
+        stats = dict(histories=st[0], seconds=st[1], launches=int(st[2]), edep=st[3], esrc=st[4],
+                     flags=int(st[5]))
+        return dose.reshape(self.shape), unc.reshape(self.shape), stats
+
+    def run_beam_noalloc(self, ncase, nbatch=10, seed=1, spectrum=None, mono_energy=1.25, charge=0, ssd=100.0,
+                         collimator=(-5.0, 5.0, -5.0, 5.0)):
+        """run_beam in the plain FP64 form on the library's fixed device
+        scratch: for callers that must not allocate device memory during the
+        run (see omc_run_beam_noalloc in include/omcgpu.h; at most
+        OMC_NOALLOC_MAX_VOXELS = 262144 voxels; concurrent calls race)."""
+        keep = []
+        b = _Beam()
+        b.energy = self._energy(spectrum, mono_energy, charge, keep)
+        b.ssd = ssd
+        b.xinl, b.xinu, b.yinl, b.yinu = collimator
+        n = int(np.prod(self.shape))
+        dose = np.zeros(n)
+        unc = np.zeros(n)
+        st = np.zeros(6)
+        _check(lib().omc_run_beam_noalloc(self.h, C.byref(b), int(ncase), int(nbatch), int(seed) & (2**64 - 1),
+                                          _p(dose, _dp), _p(unc, _dp), _p(st, _dp)), self.h)
         stats = dict(histories=st[0], seconds=st[1], launches=int(st[2]), edep=st[3], esrc=st[4],
                      flags=int(st[5]))
         return dose.reshape(self.shape), unc.reshape(self.shape), stats
