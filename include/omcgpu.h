@@ -192,16 +192,24 @@ int omc_run_beamlets(omc_engine *e, const omc_beamlets *b, int64_t nhist, int nb
 /* ------------------------------------------------------------ serving
  * Continuous batching: beam and beamlet requests of any history count are
  * admitted while device memory for their tallies is within `mem_budget`
- * bytes, and all admitted requests share the same particle queues.
- * omc_serve_* replace the sequential beamlet loop of omc_matrad.c:1576. */
+ * bytes (0: half the free memory, at most 32 GB; each request holds
+ * 10 * nvox * 8 bytes of batch tallies), at most `max_requests` (<= 256,
+ * 0 = 256) at a time; all admitted requests share the same particle
+ * queues, and requests beyond the budget wait and are admitted first come
+ * first served as earlier ones finish.  omc_server_* replace the
+ * sequential beamlet loop of omc_matrad.c:1576.  OMC_E_NOMEM when the
+ * budget holds no request. */
 typedef struct omc_server omc_server;
 int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint64_t seed, omc_server **out);
 int omc_server_destroy(omc_server *s);
 /* Submits one beamlet (index ibixel of b, which must outlive the request)
- * or one beam; returns a request id >= 0 or a negative status. */
+ * or one beam (its spectrum is copied); nbatch 2..10.  A request's random
+ * streams depend only on `seed` (0: derived from the server seed and the
+ * request id), so its result is the same alone or among other requests.
+ * Returns a request id >= 0 or a negative status. */
 int omc_server_submit_beamlet(omc_server *s, const omc_beamlets *b, int ibixel, int64_t nhist, int nbatch,
-                              double rel_threshold);
-int omc_server_submit_beam(omc_server *s, const omc_beam *b, int64_t nhist, int nbatch);
+                              double rel_threshold, uint64_t seed);
+int omc_server_submit_beam(omc_server *s, const omc_beam *b, int64_t nhist, int nbatch, uint64_t seed);
 /* Advances the device by up to `cycles` transport cycles; *active receives
  * the requests still running. */
 int omc_server_step(omc_server *s, int cycles, int *active);

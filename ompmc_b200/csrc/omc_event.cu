@@ -129,11 +129,12 @@ __device__ __forceinline__ void renorm(Part<float> &p) {
 
 // Route the event's surviving particle and its secondaries to the output
 // queues.  Secondaries get fresh streams derived from the parent's key and
-// block counter, which is unique per event.
-__device__ __forceinline__ void emit(const Queue &outP, const Queue &outE, unsigned active, bool alive,
-                                     Part<float> &p, EvEnv &g, int slot, uint32_t k0, uint32_t k1) {
+// block counter, which is unique per event.  Returns the particles queued.
+__device__ __forceinline__ int emit(const Queue &outP, const Queue &outE, unsigned active, bool alive,
+                                    Part<float> &p, EvEnv &g, int slot, uint32_t k0, uint32_t k1) {
     uint64_t pkey = ((uint64_t)k1 << 32) | k0;
     uint32_t pctr = g.rng.ctr;
+    int queued = 0;
 #pragma unroll
     for (int k = 0; k < 1 + EV_MAXOUT; k++) {
         bool has;
@@ -164,7 +165,9 @@ __device__ __forceinline__ void emit(const Queue &outP, const Queue &outE, unsig
         }
         if (ip >= 0) qstore(outP, ip, q, slot, a0, a1, ac);
         if (ie >= 0) qstore(outE, ie, q, slot, a0, a1, ac);
+        queued += (ip >= 0) + (ie >= 0);
     }
+    return queued;
 }
 
 __device__ __forceinline__ void report_flags(Ctl *ctl, unsigned flags, unsigned active) {
@@ -177,10 +180,20 @@ __device__ __forceinline__ void report_count(unsigned long long *dst, unsigned v
     if (t && (threadIdx.x & 31) == __ffs(active) - 1) atomicAdd(dst, (unsigned long long)t);
 }
 
+// Live-particle count of a serving request: +delta for the request whose
+// tally slots start at req*nbmax, aggregated over the lanes of the warp that
+// hold particles of the same request.
+__device__ __forceinline__ void add_live(int *live, int nbmax, int slot, int delta, unsigned active) {
+    int req = slot / nbmax;
+    unsigned grp = __match_any_sync(active, req);
+    int tot = __reduce_add_sync(grp, delta);
+    if (tot != 0 && (threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&live[req], tot);
+}
+
 template <bool PHOTON>
 __device__ __forceinline__ void transport_events(const DevData<float> &D, const Queue &in, const Queue &outP,
                                                  const Queue &outE, double *tallies, long nvox, Ctl *ctl,
-                                                 uint32_t seedw, int tsteps) {
+                                                 uint32_t seedw, int tsteps, int *live, int nbmax) {
     int n = min(*in.count, in.cap);
     unsigned flags = 0;
     unsigned c_ev = 0, c_steps = 0, c_cross = 0, c_dep = 0, c_atom = 0;
@@ -205,7 +218,8 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
         if (PHOTON) alive = photon_step(D, g, p);
         else alive = electron_step(D, g, p) == E_ALIVE;
         g.flush();
-        emit(outP, outE, active, alive, p, g, slot, k0, k1);
+        int emitted = emit(outP, outE, active, alive, p, g, slot, k0, k1);
+        if (live) add_live(live, nbmax, slot, emitted - 1, active);
         flags |= g.flags;
         c_ev++;
         c_steps += g.work;
@@ -223,10 +237,12 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
     report_count(&ctl->st_atom[k], c_atom, active);
 }
 
-// One photon event per queued photon.
+// One photon event per queued photon.  `live` (may be null) receives the
+// change of each serving request's live-particle count.
 __global__ void __launch_bounds__(256) k_photon_step(DevData<float> D, Queue in, Queue outP, Queue outE,
-                                                     double *tallies, long nvox, Ctl *ctl, uint32_t seedw) {
-    transport_events<true>(D, in, outP, outE, tallies, nvox, ctl, seedw, 1 << 30);
+                                                     double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
+                                                     int *live, int nbmax) {
+    transport_events<true>(D, in, outP, outE, tallies, nvox, ctl, seedw, 1 << 30, live, nbmax);
 }
 
 // One bounded electron/positron event per queued charged particle: at most
@@ -234,8 +250,8 @@ __global__ void __launch_bounds__(256) k_photon_step(DevData<float> D, Queue in,
 // re-queued, so every lane of a warp does a similar amount of work.
 __global__ void __launch_bounds__(256) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
                                                        double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
-                                                       int tsteps) {
-    transport_events<false>(D, in, outP, outE, tallies, nvox, ctl, seedw, tsteps);
+                                                       int tsteps, int *live, int nbmax) {
+    transport_events<false>(D, in, outP, outE, tallies, nvox, ctl, seedw, tsteps, live, nbmax);
 }
 
 __global__ void k_source(DevData<float> D, BeamSrc<float> S, Queue qP, Queue qE, Ctl *ctl, long long nper,
@@ -302,7 +318,7 @@ static int alloc_queue(omc_engine *e, DBuf &b, Queue &q, int cap, int *count) {
     return OMC_OK;
 }
 
-static int event_prepare(omc_engine *e) {
+int event_prepare(omc_engine *e) {
     if (e->ev && e->ev->ready) return OMC_OK;
     if (!e->ev) e->ev = new EventState();
     EventState &S = *e->ev;
@@ -342,10 +358,10 @@ static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, doubl
     k_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, src, S.q[iph], S.q[iel], S.ctl_d, nper, seed, seedw);
     if (ev) cudaEventRecord(ev[2], e->stream);
     k_photon_step<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
-                                                          S.ctl_d, seedw);
+                                                          S.ctl_d, seedw, nullptr, 1);
     if (ev) cudaEventRecord(ev[3], e->stream);
     k_electron_step<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
-                                                           S.ctl_d, seedw, S.tsteps);
+                                                           S.ctl_d, seedw, S.tsteps, nullptr, 1);
     if (ev) cudaEventRecord(ev[4], e->stream);
     k_reset<<<1, 1, 0, e->stream>>>(S.ctl_d, iph, iel);
     if (ev) cudaEventRecord(ev[5], e->stream);
@@ -497,6 +513,83 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
     // source energy
     cudaMemcpyAsync(src_energy, &S.ctl_d->src_energy, 8, cudaMemcpyDeviceToDevice, e->stream);
     return OMC_OK;
+}
+
+// ============================================================== serving
+// Histories to inject this cycle across the admitted requests, first come
+// first served, keeping `target` particles in flight.
+__global__ void k_serve_plan(ServeDev *sd, Ctl *ctl, int iph, int iel, long long target, int cap) {
+    long long occ = (long long)min(ctl->cnt[iph], cap) + min(ctl->cnt[iel], cap);
+    long long room = target - occ;
+    long long qroom = (long long)cap - max(ctl->cnt[iph], ctl->cnt[iel]);
+    if (room > qroom) room = qroom;
+    int np = 0;
+    long long cum = 0;
+    for (int k = 0; k < sd->norder && room - cum > 0; k++) {
+        int s = sd->order[k];
+        ServeReq &r = sd->req[s];
+        if (r.kind < 0) continue;
+        long long rem = r.nhist - r.next;
+        if (rem <= 0) continue;
+        long long take = rem < room - cum ? rem : room - cum;
+        sd->plan_slot[np] = s;
+        sd->plan_first[np] = r.next;
+        sd->plan_cum[np] = (int)cum;
+        cum += take;
+        r.next += take;
+        np++;
+    }
+    sd->plan_cum[np] = (int)cum;
+    sd->nplan = np;
+    sd->inject_total = (int)cum;
+}
+
+// Primaries of the planned histories; each history's stream key is derived
+// from its request's seed and its index within the request.
+__global__ void k_serve_source(DevData<float> D, ServeDev *sd, Queue qP, Queue qE, Ctl *ctl, int nbmax,
+                               uint32_t seedw) {
+    int n = sd->inject_total, np = sd->nplan;
+    unsigned flags = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        unsigned active = __activemask();
+        int lo = 0, hi = np - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (sd->plan_cum[mid] <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        int s = sd->plan_slot[lo];
+        const ServeReq &r = sd->req[s];
+        long long local = sd->plan_first[lo] + (i - sd->plan_cum[lo]);
+        uint64_t key = mix64(r.seed ^ (uint64_t)local * 0x9E3779B97F4A7C15ull);
+        SrcEnv g;
+        g.rng.init(key, seedw);
+        float ein;
+        Part<float> p = r.kind == 0 ? beam_primary(D, sd->beam[s], g, ein) : beamlet_primary(D, sd->bl[s], r.bixel, g, ein);
+        int slot = s * nbmax + (int)(local / r.nper);
+        int ip = warp_append(qP, p.iq == 0, active, flags);
+        int ie = warp_append(qE, p.iq != 0, active, flags);
+        if (ip >= 0) qstore(qP, ip, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.ctr);
+        if (ie >= 0) qstore(qE, ie, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.ctr);
+        add_live(sd->live, nbmax, slot, (ip >= 0) + (ie >= 0), active);
+    }
+    unsigned active = __activemask();
+    report_flags(ctl, flags, active);
+}
+
+void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target) {
+    EventState &S = *e->ev;
+    int iph = in == 0 ? 0 : 2, iel = iph + 1;
+    int oph = in == 0 ? 2 : 0, oel = oph + 1;
+    uint32_t seedw = 0x5e7e5eedu;
+    long nvox = e->ph.nvox();
+    k_serve_plan<<<1, 1, 0, e->stream>>>(sd, S.ctl_d, iph, iel, target, S.cap);
+    k_serve_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, sd, S.q[iph], S.q[iel], S.ctl_d, nbmax, seedw);
+    k_photon_step<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox, S.ctl_d,
+                                                      seedw, sd->live, nbmax);
+    k_electron_step<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
+                                                        S.ctl_d, seedw, S.tsteps, sd->live, nbmax);
+    k_reset<<<1, 1, 0, e->stream>>>(S.ctl_d, iph, iel);
 }
 
 }  // namespace omc

@@ -50,6 +50,39 @@ struct EventState {
     KernelProfile prof[4];    // 0 source, 1 photon, 2 electron, 3 plan+reset
 };
 
+// ------------------------------------------------------------ serving
+constexpr int SERVE_MAX = 256;  // request slots resident on the device
+
+// One admitted request: its histories are injected from `next` on; kind -1
+// marks a free slot.
+struct ServeReq {
+    int kind;            // -1 free, 0 beam, 1 beamlet
+    int bixel;
+    long long nhist, next, nper;
+    unsigned long long seed;
+};
+
+// Device-resident request table and the per-cycle injection plan.
+struct ServeDev {
+    ServeReq req[SERVE_MAX];
+    BeamSrc<float> beam[SERVE_MAX];
+    BeamletSrc<float> bl[SERVE_MAX];
+    int live[SERVE_MAX];       // particles of the request in the queues
+    int order[SERVE_MAX];      // active slots in admission order
+    int norder;
+    int nplan;
+    int inject_total;
+    int pad;
+    int plan_slot[SERVE_MAX];
+    long long plan_first[SERVE_MAX];
+    int plan_cum[SERVE_MAX + 1];
+};
+
+int event_prepare(omc_engine *e);
+// One serving cycle with input buffers `in` (0 = A, 1 = B); tally slot of a
+// particle = request slot * nbmax + batch.
+void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
+
 int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint64_t seed, double *sum, double *sum2,
                    double *src_energy, KernelStats &ks);
 void event_release(omc_engine *e);

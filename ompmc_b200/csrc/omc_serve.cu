@@ -1,0 +1,655 @@
+// Serving: continuous batching of beam and beamlet dose requests on one GPU,
+// and the matRad dose-influence entry (omc_run_beamlets) built on it.
+//
+// Admitted requests share the event form's particle queues.  Each holds a
+// device slot: a ServeReq entry, a source descriptor and nbatch FP64 working
+// tallies.  Every transport cycle a planner kernel hands out injection room
+// first come first served; the transport kernels keep a live-particle count
+// per request.  A request is finished when all its histories are injected and
+// its live count is zero; the host then folds its batch tallies, finalises
+// dose and uncertainty (matRad: variance of the mean), extracts the sparse
+// column (entries above rel_threshold * column maximum, rows ascending), frees
+// the slot and admits the next pending request.  The sequential beamlet loop
+// it replaces is omc_matrad.c:1576-1720.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+
+#include "omc_event.h"
+#include "omc_rng.cuh"
+#include "omc_source.cuh"
+
+namespace omc {
+int finalize_dosxyz(omc_engine *e, const double *sum, const double *sum2, int nbatch, double nper, double *dose,
+                    double *unc);
+int finalize_matrad(omc_engine *e, const double *sum, const double *sum2, int nbatch, double *dose, double *var);
+
+// ----------------------------------------------- sparse column extraction
+constexpr int NSEG = 1024;
+
+__global__ void k_dmax(const double *d, long n, unsigned long long *out) {
+    double m = 0.0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        m = fmax(m, d[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    // dose is non-negative: the IEEE bit pattern orders like the value
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+__device__ __forceinline__ double thresh_of(const unsigned long long *dmaxbits, double rel) {
+    return __longlong_as_double((long long)*dmaxbits) * rel;
+}
+
+// Entries above the threshold per contiguous segment of voxels.
+__global__ void k_seg_count(const double *d, long n, long seglen, const unsigned long long *dmaxbits, double rel,
+                            int *counts) {
+    __shared__ int red[32];
+    double t = thresh_of(dmaxbits, rel);
+    long lo = (long)blockIdx.x * seglen, hi = min(n, lo + seglen);
+    int c = 0;
+    for (long i = lo + threadIdx.x; i < hi; i += blockDim.x) c += d[i] > t;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        c = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0;
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+        if (threadIdx.x == 0) counts[blockIdx.x] = c;
+    }
+}
+
+// Exclusive scan of the NSEG segment counts (one block of NSEG threads).
+__global__ void k_seg_scan(const int *counts, int *offsets, long long *total) {
+    __shared__ int s[NSEG];
+    int i = threadIdx.x;
+    s[i] = counts[i];
+    __syncthreads();
+    for (int o = 1; o < NSEG; o <<= 1) {
+        int v = i >= o ? s[i - o] : 0;
+        __syncthreads();
+        s[i] += v;
+        __syncthreads();
+    }
+    offsets[i] = s[i] - counts[i];
+    if (i == NSEG - 1) *total = s[i];
+}
+
+// Ordered compaction: each segment writes its entries at its offset, in
+// voxel order, a block-wide tile at a time.
+__global__ void k_seg_write(const double *d, const double *v, long n, long seglen, const unsigned long long *dmaxbits,
+                            double rel, const int *offsets, int *rows, double *vals, double *vars, long long cap) {
+    __shared__ int wsum[32];
+    double t = thresh_of(dmaxbits, rel);
+    long lo = (long)blockIdx.x * seglen, hi = min(n, lo + seglen);
+    long long base = offsets[blockIdx.x];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (long t0 = lo; t0 < hi; t0 += blockDim.x) {
+        long i = t0 + threadIdx.x;
+        bool keep = i < hi && d[i] > t;
+        unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) wsum[wid] = __popc(m);
+        __syncthreads();
+        int before = 0, tile = 0;
+        for (int w = 0; w < nw; w++) {
+            before += w < wid ? wsum[w] : 0;
+            tile += wsum[w];
+        }
+        if (keep) {
+            long long o = base + before + __popc(m & ((1u << lane) - 1));
+            if (o < cap) {
+                rows[o] = (int)i;
+                vals[o] = d[i];
+                if (vars) vars[o] = v[i];
+            }
+        }
+        base += tile;
+        __syncthreads();
+    }
+}
+
+}  // namespace omc
+
+using namespace omc;
+
+namespace {
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Device copy of a beamlet set, in FP32 for the event form and FP64 for the
+// plain form.
+struct PlanBuf {
+    DBuf f32, f64;
+    BeamletSrc<float> s32{};
+    BeamletSrc<double> s64{};
+};
+
+template <typename R>
+int upload_plan(omc_engine *e, const omc_beamlets *b, DBuf &buf, BeamletSrc<R> &s) {
+    int nb = b->nbixels, nbeams = b->nbeams, ncdf = b->energy.n;
+    size_t nr = (size_t)3 * nbeams + 9 * (size_t)nb + 2 * (size_t)ncdf;
+    std::vector<R> v;
+    v.reserve(nr);
+    for (int i = 0; i < 3 * nbeams; i++) v.push_back((R)b->src[i]);
+    for (int i = 0; i < 3 * nb; i++) v.push_back((R)b->corner[i]);
+    for (int i = 0; i < 3 * nb; i++) v.push_back((R)b->side1[i]);
+    for (int i = 0; i < 3 * nb; i++) v.push_back((R)b->side2[i]);
+    for (int i = 0; i < ncdf; i++) v.push_back((R)b->energy.cdf1[i]);
+    for (int i = 0; i < ncdf; i++) v.push_back((R)b->energy.cdf2[i]);
+    size_t bytes = v.size() * sizeof(R) + (size_t)nb * 4 + 256;
+    int rc = buf.alloc(bytes);
+    if (rc) return set_err(e, rc, "beamlet set allocation failed");
+    cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(R), cudaMemcpyHostToDevice, e->stream);
+    size_t ioff = ((v.size() * sizeof(R)) + 255) / 256 * 256;
+    int *ib = (int *)((char *)buf.p + ioff);
+    cudaMemcpyAsync(ib, b->ibeam, (size_t)nb * 4, cudaMemcpyHostToDevice, e->stream);
+    R *p = (R *)buf.p;
+    s = BeamletSrc<R>{};
+    s.charge = b->energy.charge;
+    s.spectrum = ncdf > 0 ? 1 : 0;
+    s.gaussian = b->gaussian ? 1 : 0;
+    s.energy = (R)b->energy.mono_energy;
+    s.gauss_width = (R)b->gauss_width;
+    s.src = p;
+    s.corner = p + 3 * nbeams;
+    s.side1 = p + 3 * nbeams + 3 * (size_t)nb;
+    s.side2 = p + 3 * nbeams + 6 * (size_t)nb;
+    s.cdf1 = ncdf > 0 ? p + 3 * nbeams + 9 * (size_t)nb : nullptr;
+    s.cdf2 = ncdf > 0 ? p + 3 * nbeams + 9 * (size_t)nb + ncdf : nullptr;
+    s.deltak = (R)ncdf;
+    s.ibeam = ib;
+    return OMC_OK;
+}
+
+int check_beamlets(omc_engine *e, const omc_beamlets *b) {
+    if (!b || b->nbixels <= 0 || b->nbeams <= 0 || !b->ibeam || !b->src || !b->corner || !b->side1 || !b->side2)
+        return set_err(e, OMC_E_ARG, "incomplete beamlet description");
+    if (b->energy.n > 0 && (!b->energy.cdf1 || !b->energy.cdf2)) return set_err(e, OMC_E_ARG, "spectrum arrays missing");
+    for (int i = 0; i < b->nbixels; i++)
+        if (b->ibeam[i] < 0 || b->ibeam[i] >= b->nbeams) return set_err(e, OMC_E_ARG, "beamlet beam index out of range");
+    return OMC_OK;
+}
+
+struct Request {
+    int id = -1, kind = 0, slot = -1, state = 0;  // state 0 pending, 1 running, 2 done, 3 released
+    long long nhist = 0, nper = 0;
+    int nbatch = 0, bixel = 0;
+    double rel = 0;
+    const omc_beamlets *bl = nullptr;
+    omc_beam beam{};
+    DBuf cdf;
+    double t_submit = 0, t_done = 0;
+    std::vector<int32_t> rows;
+    std::vector<double> vals, var, dose, unc;
+    uint64_t seed = 0;
+};
+
+}  // namespace
+
+struct omc_server {
+    omc_engine *e = nullptr;
+    int nbmax = 10, nslots = 0;
+    long long target = 0;
+    uint64_t seed = 0;
+    DBuf tallies, sdbuf, fin;
+    ServeDev *sd = nullptr;
+    std::vector<std::unique_ptr<Request>> reqs;
+    std::deque<int> pending;
+    std::vector<int> slot_req;   // request id per slot, -1 free
+    std::vector<int> order;      // running slots in admission order
+    std::map<const omc_beamlets *, std::unique_ptr<PlanBuf>> plans;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long cycles = 0;
+    // finalise scratch (device): sum, sum2, dose, var | rows | vals | vars | seg counts/offsets | dmax | total
+    double *f_sum = nullptr, *f_sum2 = nullptr, *f_dose = nullptr, *f_var = nullptr, *f_vals = nullptr,
+           *f_vars = nullptr;
+    int *f_rows = nullptr, *f_cnt = nullptr, *f_off = nullptr;
+    unsigned long long *f_dmax = nullptr;
+    long long *f_total = nullptr;
+};
+
+namespace {
+
+// Fold, finalise and extract one finished request into host memory.
+int finalize_request(omc_server *s, Request &r) {
+    omc_engine *e = s->e;
+    long nv = e->ph.nvox();
+    int rc;
+    cudaMemsetAsync(s->f_sum, 0, nv * 8, e->stream);
+    cudaMemsetAsync(s->f_sum2, 0, nv * 8, e->stream);
+    double scale = r.kind == 1 ? 1.0 / (double)r.nper : 1.0;
+    for (int b = 0; b < r.nbatch; b++) {
+        double *w = s->tallies.as<double>() + ((size_t)r.slot * s->nbmax + b) * nv;
+        if ((rc = fold(e, w, s->f_sum, s->f_sum2, nv, scale))) return rc;
+    }
+    if (r.kind == 0) {
+        if ((rc = finalize_dosxyz(e, s->f_sum, s->f_sum2, r.nbatch, (double)r.nper, s->f_dose, s->f_var))) return rc;
+        r.dose.resize(nv);
+        r.unc.resize(nv);
+        cudaMemcpyAsync(r.dose.data(), s->f_dose, nv * 8, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpyAsync(r.unc.data(), s->f_var, nv * 8, cudaMemcpyDeviceToHost, e->stream);
+        return cuda_check(e, cudaStreamSynchronize(e->stream), "finalize beam request");
+    }
+    if ((rc = finalize_matrad(e, s->f_sum, s->f_sum2, r.nbatch, s->f_dose, s->f_var))) return rc;
+    cudaMemsetAsync(s->f_dmax, 0, 8, e->stream);
+    int g = std::max(1, std::min((int)((nv + 255) / 256), e->sm_count * 4));
+    k_dmax<<<g, 256, 0, e->stream>>>(s->f_dose, nv, s->f_dmax);
+    long seglen = (nv + NSEG - 1) / NSEG;
+    k_seg_count<<<NSEG, 256, 0, e->stream>>>(s->f_dose, nv, seglen, s->f_dmax, r.rel, s->f_cnt);
+    k_seg_scan<<<1, NSEG, 0, e->stream>>>(s->f_cnt, s->f_off, s->f_total);
+    k_seg_write<<<NSEG, 256, 0, e->stream>>>(s->f_dose, s->f_var, nv, seglen, s->f_dmax, r.rel, s->f_off, s->f_rows,
+                                              s->f_vals, s->f_vars, nv);
+    if ((rc = cuda_check(e, cudaGetLastError(), "sparse extraction"))) return rc;
+    long long nnz = 0;
+    cudaMemcpyAsync(&nnz, s->f_total, 8, cudaMemcpyDeviceToHost, e->stream);
+    if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "sparse count"))) return rc;
+    r.rows.resize(nnz);
+    r.vals.resize(nnz);
+    r.var.resize(nnz);
+    if (nnz > 0) {
+        cudaMemcpyAsync(r.rows.data(), s->f_rows, nnz * 4, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpyAsync(r.vals.data(), s->f_vals, nnz * 8, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpyAsync(r.var.data(), s->f_vars, nnz * 8, cudaMemcpyDeviceToHost, e->stream);
+    }
+    return cuda_check(e, cudaStreamSynchronize(e->stream), "sparse column");
+}
+
+int admit(omc_server *s) {
+    omc_engine *e = s->e;
+    bool changed = false;
+    while (!s->pending.empty()) {
+        int slot = -1;
+        for (int k = 0; k < s->nslots; k++)
+            if (s->slot_req[k] < 0) { slot = k; break; }
+        if (slot < 0) break;
+        Request &r = *s->reqs[s->pending.front()];
+        s->pending.pop_front();
+        r.slot = slot;
+        r.state = 1;
+        s->slot_req[slot] = r.id;
+        s->order.push_back(slot);
+        ServeReq q{};
+        q.kind = r.kind;
+        q.bixel = r.bixel;
+        q.nhist = r.nhist;
+        q.next = 0;
+        q.nper = r.nper;
+        q.seed = r.seed;
+        cudaMemcpyAsync(&s->sd->req[slot], &q, sizeof(q), cudaMemcpyHostToDevice, e->stream);
+        if (r.kind == 0) {
+            BeamSrc<float> b = beam_setup<float>(e, &r.beam);
+            if (r.beam.energy.n > 0) {
+                b.cdf1 = r.cdf.as<float>();
+                b.cdf2 = r.cdf.as<float>() + r.beam.energy.n;
+            }
+            cudaMemcpyAsync(&s->sd->beam[slot], &b, sizeof(b), cudaMemcpyHostToDevice, e->stream);
+        } else {
+            cudaMemcpyAsync(&s->sd->bl[slot], &s->plans[r.bl]->s32, sizeof(BeamletSrc<float>), cudaMemcpyHostToDevice,
+                            e->stream);
+        }
+        cudaMemsetAsync(&s->sd->live[slot], 0, sizeof(int), e->stream);
+        changed = true;
+    }
+    if (changed) {
+        int n = (int)s->order.size();
+        cudaMemcpyAsync(s->sd->order, s->order.data(), n * sizeof(int), cudaMemcpyHostToDevice, e->stream);
+        cudaMemcpyAsync(&s->sd->norder, &n, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+        return cuda_check(e, cudaStreamSynchronize(e->stream), "admission");
+    }
+    return OMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint64_t seed, omc_server **out) {
+    if (!e || !out) return OMC_E_ARG;
+    *out = nullptr;
+    cudaSetDevice(e->device);
+    int rc = event_prepare(e);
+    if (rc) return rc;
+    auto s = std::make_unique<omc_server>();
+    s->e = e;
+    s->seed = seed;
+    long nv = e->ph.nvox();
+    size_t per_slot = (size_t)s->nbmax * nv * 8;
+    if (mem_budget <= 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        mem_budget = (int64_t)std::min<size_t>(fr / 2, (size_t)32 << 30);
+    }
+    long long fit = (long long)(mem_budget / (int64_t)per_slot);
+    if (max_requests <= 0) max_requests = SERVE_MAX;
+    s->nslots = (int)std::min<long long>(std::min(fit, (long long)max_requests), SERVE_MAX);
+    if (s->nslots < 1)
+        return set_err(e, OMC_E_NOMEM, "memory budget holds no request's tallies (" + std::to_string(per_slot) +
+                                           " bytes each)");
+    if ((rc = s->tallies.alloc(per_slot * s->nslots))) return set_err(e, rc, "server tally allocation failed");
+    cudaMemsetAsync(s->tallies.p, 0, per_slot * s->nslots, e->stream);
+    if ((rc = s->sdbuf.alloc(sizeof(ServeDev)))) return set_err(e, rc, "server table allocation failed");
+    s->sd = s->sdbuf.as<ServeDev>();
+    cudaMemsetAsync(s->sd, 0, sizeof(ServeDev), e->stream);
+    {
+        std::vector<ServeReq> free_req(SERVE_MAX);
+        for (auto &q : free_req) q.kind = -1;
+        cudaMemcpyAsync(s->sd->req, free_req.data(), sizeof(ServeReq) * SERVE_MAX, cudaMemcpyHostToDevice, e->stream);
+    }
+    size_t fin = (size_t)nv * (8 * 6 + 4) + NSEG * 8 + 64;
+    if ((rc = s->fin.alloc(fin))) return set_err(e, rc, "server finalize allocation failed");
+    double *f = s->fin.as<double>();
+    s->f_sum = f;
+    s->f_sum2 = f + nv;
+    s->f_dose = f + 2 * nv;
+    s->f_var = f + 3 * nv;
+    s->f_vals = f + 4 * nv;
+    s->f_vars = f + 5 * nv;
+    s->f_rows = (int *)(f + 6 * nv);
+    s->f_cnt = s->f_rows + nv;
+    s->f_off = s->f_cnt + NSEG;
+    s->f_dmax = (unsigned long long *)(((uintptr_t)(s->f_off + NSEG) + 15) / 16 * 16);
+    s->f_total = (long long *)(s->f_dmax + 1);
+    s->slot_req.assign(s->nslots, -1);
+    s->target = std::min<long long>((long long)e->ev->cap / 2, e->ev->inflight);
+    // reset queue counters and capture two cycles as a graph
+    Ctl c0{};
+    cudaMemcpyAsync(e->ev->ctl_d, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, e->stream);
+    if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "server init"))) return rc;
+    if ((rc = cuda_check(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal), "capture")))
+        return rc;
+    serve_launch_cycle(e, 0, s->sd, s->tallies.as<double>(), s->nbmax, s->target);
+    serve_launch_cycle(e, 1, s->sd, s->tallies.as<double>(), s->nbmax, s->target);
+    if ((rc = cuda_check(e, cudaStreamEndCapture(e->stream, &s->graph), "end capture"))) return rc;
+    if ((rc = cuda_check(e, cudaGraphInstantiate(&s->exec, s->graph, 0), "graph instantiate"))) return rc;
+    *out = s.release();
+    return OMC_OK;
+}
+
+int omc_server_destroy(omc_server *s) {
+    if (!s) return OMC_OK;
+    cudaSetDevice(s->e->device);
+    cudaStreamSynchronize(s->e->stream);
+    if (s->exec) cudaGraphExecDestroy(s->exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    delete s;
+    return OMC_OK;
+}
+
+static int submit(omc_server *s, std::unique_ptr<Request> r, uint64_t seed) {
+    if (r->nbatch < 2 || r->nbatch > s->nbmax)
+        return set_err(s->e, OMC_E_RANGE, "nbatch must be 2.." + std::to_string(s->nbmax));
+    if (r->nhist / r->nbatch == 0) r->nhist = r->nbatch;
+    r->nper = r->nhist / r->nbatch;
+    r->nhist = r->nper * r->nbatch;
+    r->id = (int)s->reqs.size();
+    r->seed = seed ? mix64(seed) : mix64(s->seed ^ ((uint64_t)(r->id + 1) * 0xD1B54A32D192ED03ull));
+    r->t_submit = now_ms();
+    int id = r->id;
+    s->reqs.push_back(std::move(r));
+    s->pending.push_back(id);
+    return id;
+}
+
+int omc_server_submit_beamlet(omc_server *s, const omc_beamlets *b, int ibixel, int64_t nhist, int nbatch,
+                              double rel_threshold, uint64_t seed) {
+    if (!s || !b) return OMC_E_ARG;
+    int rc = check_beamlets(s->e, b);
+    if (rc) return rc;
+    if (ibixel < 0 || ibixel >= b->nbixels) return set_err(s->e, OMC_E_ARG, "bixel index out of range");
+    if (!s->plans.count(b)) {
+        auto p = std::make_unique<PlanBuf>();
+        if ((rc = upload_plan<float>(s->e, b, p->f32, p->s32))) return rc;
+        s->plans[b] = std::move(p);
+    }
+    auto r = std::make_unique<Request>();
+    r->kind = 1;
+    r->bl = b;
+    r->bixel = ibixel;
+    r->nhist = nhist;
+    r->nbatch = nbatch;
+    r->rel = rel_threshold;
+    return submit(s, std::move(r), seed);
+}
+
+int omc_server_submit_beam(omc_server *s, const omc_beam *b, int64_t nhist, int nbatch, uint64_t seed) {
+    if (!s || !b) return OMC_E_ARG;
+    auto r = std::make_unique<Request>();
+    r->kind = 0;
+    r->beam = *b;
+    int n = b->energy.n;
+    if (n > 0) {
+        if (!b->energy.cdf1 || !b->energy.cdf2) return set_err(s->e, OMC_E_ARG, "spectrum arrays missing");
+        std::vector<float> c(b->energy.cdf1, b->energy.cdf1 + n);
+        c.insert(c.end(), b->energy.cdf2, b->energy.cdf2 + n);
+        int rc = r->cdf.alloc(c.size() * 4);
+        if (rc) return set_err(s->e, rc, "alloc");
+        cudaMemcpy(r->cdf.p, c.data(), c.size() * 4, cudaMemcpyHostToDevice);
+        r->beam.energy.cdf1 = r->beam.energy.cdf2 = nullptr;  // host arrays are not kept
+    }
+    r->nhist = nhist;
+    r->nbatch = nbatch;
+    return submit(s, std::move(r), seed);
+}
+
+int omc_server_step(omc_server *s, int cycles, int *active) {
+    if (!s) return OMC_E_ARG;
+    omc_engine *e = s->e;
+    cudaSetDevice(e->device);
+    int rc = admit(s);
+    if (rc) return rc;
+    if (!s->order.empty()) {
+        int graphs = std::max(1, cycles / 2);
+        for (int k = 0; k < graphs; k++) cudaGraphLaunch(s->exec, e->stream);
+        s->cycles += 2 * graphs;
+        // completion check: all injected and nothing left in the queues
+        std::vector<ServeReq> rq(s->nslots);
+        std::vector<int> live(s->nslots);
+        unsigned flags = 0;
+        cudaMemcpyAsync(rq.data(), s->sd->req, sizeof(ServeReq) * s->nslots, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpyAsync(live.data(), s->sd->live, sizeof(int) * s->nslots, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpyAsync(&flags, &e->ev->ctl_d->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream);
+        if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "server step"))) return rc;
+        if (flags & (ERR_QUEUE | ERR_NAN | ERR_STACK))
+            return set_err(e, OMC_E_DEVICE, "device error flags " + std::to_string(flags) + " in serving");
+        std::vector<int> keep;
+        bool freed = false;
+        for (int slot : s->order) {
+            Request &r = *s->reqs[s->slot_req[slot]];
+            if (rq[slot].next >= r.nhist && live[slot] == 0) {
+                if ((rc = finalize_request(s, r))) return rc;
+                r.state = 2;
+                r.t_done = now_ms();
+                s->slot_req[slot] = -1;
+                ServeReq q{};
+                q.kind = -1;
+                cudaMemcpyAsync(&s->sd->req[slot], &q, sizeof(q), cudaMemcpyHostToDevice, e->stream);
+                freed = true;
+            } else {
+                keep.push_back(slot);
+            }
+        }
+        if (freed) {
+            s->order = keep;
+            int n = (int)s->order.size();
+            if (n) cudaMemcpyAsync(s->sd->order, s->order.data(), n * sizeof(int), cudaMemcpyHostToDevice, e->stream);
+            cudaMemcpyAsync(&s->sd->norder, &n, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+            if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "server release"))) return rc;
+            if ((rc = admit(s))) return rc;
+        }
+    }
+    if (active) *active = (int)(s->order.size() + s->pending.size());
+    return OMC_OK;
+}
+
+int omc_server_poll(omc_server *s, int id, double *latency_ms) {
+    if (!s || id < 0 || id >= (int)s->reqs.size()) return OMC_E_ARG;
+    Request &r = *s->reqs[id];
+    if (r.state < 2) return OMC_E_NOTREADY;
+    if (latency_ms) *latency_ms = r.t_done - r.t_submit;
+    return OMC_OK;
+}
+
+int omc_server_result_sparse(omc_server *s, int id, int32_t *rows, double *vals, double *var, int64_t cap,
+                             int64_t *nnz) {
+    if (!s || id < 0 || id >= (int)s->reqs.size() || !nnz) return OMC_E_ARG;
+    Request &r = *s->reqs[id];
+    if (r.state < 2) return OMC_E_NOTREADY;
+    if (r.kind != 1) return set_err(s->e, OMC_E_ARG, "request is not a beamlet");
+    *nnz = (int64_t)r.rows.size();
+    if ((int64_t)r.rows.size() > cap) return OMC_E_RANGE;
+    if (rows) std::copy(r.rows.begin(), r.rows.end(), rows);
+    if (vals) std::copy(r.vals.begin(), r.vals.end(), vals);
+    if (var) std::copy(r.var.begin(), r.var.end(), var);
+    return OMC_OK;
+}
+
+int omc_server_result_dense(omc_server *s, int id, double *dose, double *unc) {
+    if (!s || id < 0 || id >= (int)s->reqs.size()) return OMC_E_ARG;
+    Request &r = *s->reqs[id];
+    if (r.state < 2) return OMC_E_NOTREADY;
+    if (r.kind != 0) return set_err(s->e, OMC_E_ARG, "request is not a beam");
+    if (dose) std::copy(r.dose.begin(), r.dose.end(), dose);
+    if (unc) std::copy(r.unc.begin(), r.unc.end(), unc);
+    return OMC_OK;
+}
+
+int omc_server_release(omc_server *s, int id) {
+    if (!s || id < 0 || id >= (int)s->reqs.size()) return OMC_E_ARG;
+    Request &r = *s->reqs[id];
+    if (r.state < 2) return OMC_E_NOTREADY;
+    r.state = 3;
+    std::vector<int32_t>().swap(r.rows);
+    std::vector<double>().swap(r.vals);
+    std::vector<double>().swap(r.var);
+    std::vector<double>().swap(r.dose);
+    std::vector<double>().swap(r.unc);
+    return OMC_OK;
+}
+
+// ------------------------------------------------------- matRad D_ij
+int omc_run_beamlets(omc_engine *e, const omc_beamlets *b, int64_t nhist, int nbatch, double rel_threshold,
+                     uint64_t seed, int mode, int64_t *colptr, int32_t *rows, double *vals, double *var, int64_t cap,
+                     int64_t *nnz, double *stats) {
+    if (!e || !b || !colptr || !nnz) return OMC_E_ARG;
+    int rc = check_beamlets(e, b);
+    if (rc) return rc;
+    if (nbatch < 2) return set_err(e, OMC_E_ARG, "nbatch must be >= 2");
+    cudaSetDevice(e->device);
+    int nb = b->nbixels;
+    std::vector<std::vector<int32_t>> cr(nb);
+    std::vector<std::vector<double>> cv(nb), cvar(nb);
+    double t0 = now_ms();
+    long long histories = 0;
+    double launches = 0;
+    if (mode == OMC_EVENT_FP32) {
+        if (nbatch > 10) return set_err(e, OMC_E_RANGE, "the event form supports nbatch <= 10");
+        omc_server *s = nullptr;
+        if ((rc = omc_server_create(e, 0, 0, seed, &s))) return rc;
+        std::unique_ptr<omc_server, int (*)(omc_server *)> guard(s, omc_server_destroy);
+        std::vector<int> ids(nb);
+        for (int i = 0; i < nb; i++) {
+            ids[i] = omc_server_submit_beamlet(s, b, i, nhist, nbatch, rel_threshold,
+                                               mix64(seed ^ ((uint64_t)(i + 1) * 0x9E3779B97F4A7C15ull)));
+            if (ids[i] < 0) return ids[i];
+        }
+        int active = nb;
+        long long guard_cycles = 0;
+        while (active > 0) {
+            if ((rc = omc_server_step(s, 8, &active))) return rc;
+            if (++guard_cycles > 10000000) return set_err(e, OMC_E_DEVICE, "serving did not drain");
+        }
+        for (int i = 0; i < nb; i++) {
+            Request &r = *s->reqs[ids[i]];
+            cr[i] = std::move(r.rows);
+            cv[i] = std::move(r.vals);
+            cvar[i] = std::move(r.var);
+            histories += r.nhist;
+        }
+        launches = (double)s->cycles * 5;
+    } else if (mode == OMC_PLAIN_FP64) {
+        PlanBuf pb;
+        if ((rc = upload_plan<double>(e, b, pb.f64, pb.s64))) return rc;
+        long nv = e->ph.nvox();
+        DBuf work, fin;
+        if ((rc = work.alloc(nv * 8))) return set_err(e, rc, "alloc");
+        size_t finb = (size_t)nv * (8 * 6 + 4) + NSEG * 8 + 64;
+        if ((rc = fin.alloc(finb))) return set_err(e, rc, "alloc");
+        cudaMemsetAsync(work.p, 0, nv * 8, e->stream);
+        double *f = fin.as<double>();
+        double *sum = f, *sum2 = f + nv, *dose = f + 2 * nv, *vv = f + 3 * nv, *fvals = f + 4 * nv, *fvars = f + 5 * nv;
+        int *frows = (int *)(f + 6 * nv), *cnt = frows + nv, *off = cnt + NSEG;
+        unsigned long long *dmax = (unsigned long long *)(((uintptr_t)(off + NSEG) + 15) / 16 * 16);
+        long long *total = (long long *)(dmax + 1);
+        if (nhist / nbatch == 0) nhist = nbatch;
+        long nper = (long)(nhist / nbatch);
+        int block = e->opt.block > 0 ? e->opt.block : 128;
+        // ompMC keeps accumulating sum2 over beamlets (omc_matrad.c:1702 resets
+        // only accum_endep): reproduced with ref_compat
+        cudaMemsetAsync(sum2, 0, nv * 8, e->stream);
+        for (int i = 0; i < nb; i++) {
+            cudaMemsetAsync(sum, 0, nv * 8, e->stream);
+            if (!e->opt.ref_compat) cudaMemsetAsync(sum2, 0, nv * 8, e->stream);
+            for (int bt = 0; bt < nbatch; bt++) {
+                if ((rc = plain_beamlet_batch(e, pb.s64, i, work.as<double>(), seed, (long)bt * nper, nper, block)))
+                    return rc;
+                if ((rc = fold(e, work.as<double>(), sum, sum2, nv, 1.0 / (double)nper))) return rc;
+            }
+            if ((rc = finalize_matrad(e, sum, sum2, nbatch, dose, vv))) return rc;
+            cudaMemsetAsync(dmax, 0, 8, e->stream);
+            int g = std::max(1, std::min((int)((nv + 255) / 256), e->sm_count * 4));
+            k_dmax<<<g, 256, 0, e->stream>>>(dose, nv, dmax);
+            long seglen = (nv + NSEG - 1) / NSEG;
+            k_seg_count<<<NSEG, 256, 0, e->stream>>>(dose, nv, seglen, dmax, rel_threshold, cnt);
+            k_seg_scan<<<1, NSEG, 0, e->stream>>>(cnt, off, total);
+            k_seg_write<<<NSEG, 256, 0, e->stream>>>(dose, vv, nv, seglen, dmax, rel_threshold, off, frows, fvals,
+                                                      fvars, nv);
+            long long n = 0;
+            cudaMemcpyAsync(&n, total, 8, cudaMemcpyDeviceToHost, e->stream);
+            if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "plain beamlet"))) return rc;
+            cr[i].resize(n);
+            cv[i].resize(n);
+            cvar[i].resize(n);
+            if (n) {
+                cudaMemcpy(cr[i].data(), frows, n * 4, cudaMemcpyDeviceToHost);
+                cudaMemcpy(cv[i].data(), fvals, n * 8, cudaMemcpyDeviceToHost);
+                cudaMemcpy(cvar[i].data(), fvars, n * 8, cudaMemcpyDeviceToHost);
+            }
+            histories += (long long)nper * nbatch;
+            launches += 2.0 * nbatch + 5;
+        }
+        unsigned flags = 0;
+        cudaMemcpy(&flags, e->errword.p, sizeof(unsigned), cudaMemcpyDeviceToHost);
+        if (flags & (ERR_STACK | ERR_NAN)) return set_err(e, OMC_E_DEVICE, "device error flags in plain beamlets");
+    } else {
+        return set_err(e, OMC_E_ARG, "unknown mode");
+    }
+    int64_t total = 0;
+    colptr[0] = 0;
+    for (int i = 0; i < nb; i++) {
+        total += (int64_t)cr[i].size();
+        colptr[i + 1] = total;
+    }
+    *nnz = total;
+    if (stats) {
+        stats[0] = (double)histories;
+        stats[1] = (now_ms() - t0) * 1e-3;
+        stats[2] = launches;
+        stats[3] = stats[4] = stats[5] = 0;
+    }
+    if (total > cap) return set_err(e, OMC_E_RANGE, "sparse capacity " + std::to_string(cap) + " < " + std::to_string(total));
+    int64_t o = 0;
+    for (int i = 0; i < nb; i++) {
+        if (rows) std::copy(cr[i].begin(), cr[i].end(), rows + o);
+        if (vals) std::copy(cv[i].begin(), cv[i].end(), vals + o);
+        if (var) std::copy(cvar[i].begin(), cvar[i].end(), var + o);
+        o += (int64_t)cr[i].size();
+    }
+    return OMC_OK;
+}
+
+}  // extern "C"

@@ -101,6 +101,16 @@ def lib():
         "omc_profile_last": ([C.c_void_p, _dp, C.c_int], C.c_int),
         "omc_run_beam_noalloc": ([C.c_void_p, C.POINTER(_Beam), C.c_int64, C.c_int, C.c_uint64, _dp, _dp, _dp],
                                  C.c_int),
+        "omc_server_create": ([C.c_void_p, C.c_int64, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)], C.c_int),
+        "omc_server_destroy": ([C.c_void_p], C.c_int),
+        "omc_server_submit_beamlet": ([C.c_void_p, C.POINTER(_Beamlets), C.c_int, C.c_int64, C.c_int, C.c_double,
+                                       C.c_uint64], C.c_int),
+        "omc_server_submit_beam": ([C.c_void_p, C.POINTER(_Beam), C.c_int64, C.c_int, C.c_uint64], C.c_int),
+        "omc_server_step": ([C.c_void_p, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "omc_server_poll": ([C.c_void_p, C.c_int, _dp], C.c_int),
+        "omc_server_result_sparse": ([C.c_void_p, C.c_int, _ip, _dp, _dp, C.c_int64, _lp], C.c_int),
+        "omc_server_result_dense": ([C.c_void_p, C.c_int, _dp, _dp], C.c_int),
+        "omc_server_release": ([C.c_void_p, C.c_int], C.c_int),
         "omc_trace_rays": ([C.c_void_p, _dp, C.c_int, C.c_int, _dp, _ip, _ip, _ip, _dp], C.c_int),
         "omc_replay": ([C.c_void_p, _dp, C.c_int, _dp, _lp, C.c_int, _ip, _dp, _ip, _lp, _up], C.c_int),
     }
@@ -356,3 +366,118 @@ class Engine:
 def dosxyz(inp_base, out_name, mode=EVENT_FP32, verbose=False):
     """The omc_dosxyz program: `<inp_base>.inp` in, `.3ddose` out."""
     _check(lib().omc_dosxyz_run(str(inp_base).encode(), str(out_name).encode(), mode, 1 if verbose else 0))
+
+
+class Server:
+    """Continuous batching of beamlet / beam requests on one engine
+    (omc_server_* in include/omcgpu.h): requests are admitted while their
+    tallies fit `mem_budget` bytes and share the engine's particle queues."""
+
+    def __init__(self, engine: Engine, mem_budget=0, max_requests=0, seed=1):
+        self.engine = engine
+        h = C.c_void_p()
+        _check(lib().omc_server_create(engine.h, int(mem_budget), int(max_requests), int(seed), C.byref(h)),
+               engine.h)
+        self.h = h
+        self._keep = {}
+
+    def beamlet_set(self, beamlets: dict):
+        """Device-side description of a beamlet set; keep the returned
+        object alive while its requests run."""
+        keep = []
+        b = Engine._beamlets_struct(beamlets, keep)
+        self._keep[id(b)] = (b, keep)
+        return b
+
+    def submit_beamlet(self, bset, ibixel, nhist, nbatch=10, rel_threshold=1e-4, seed=0):
+        rid = lib().omc_server_submit_beamlet(self.h, C.byref(bset), int(ibixel), int(nhist), int(nbatch),
+                                              float(rel_threshold), int(seed))
+        if rid < 0:
+            _check(rid, self.engine.h)
+        return rid
+
+    def submit_beam(self, ncase, nbatch=10, spectrum=None, mono_energy=1.25, charge=0, ssd=100.0,
+                    collimator=(-5.0, 5.0, -5.0, 5.0), seed=0):
+        keep = []
+        b = _Beam()
+        b.energy = Engine._energy(spectrum, mono_energy, charge, keep)
+        b.ssd = ssd
+        b.xinl, b.xinu, b.yinl, b.yinu = collimator
+        rid = lib().omc_server_submit_beam(self.h, C.byref(b), int(ncase), int(nbatch), int(seed))
+        if rid < 0:
+            _check(rid, self.engine.h)
+        return rid
+
+    def step(self, cycles=8):
+        active = C.c_int()
+        _check(lib().omc_server_step(self.h, int(cycles), C.byref(active)), self.engine.h)
+        return active.value
+
+    def poll(self, rid):
+        lat = C.c_double()
+        rc = lib().omc_server_poll(self.h, int(rid), C.byref(lat))
+        if rc == -14:
+            return None
+        _check(rc, self.engine.h)
+        return lat.value
+
+    def result_sparse(self, rid):
+        nnz = C.c_int64()
+        lib().omc_server_result_sparse(self.h, int(rid), None, None, None, 0, C.byref(nnz))
+        n = nnz.value
+        rows = np.zeros(max(n, 1), dtype=np.int32)
+        vals = np.zeros(max(n, 1))
+        var = np.zeros(max(n, 1))
+        _check(lib().omc_server_result_sparse(self.h, int(rid), _p(rows, _ip), _p(vals, _dp), _p(var, _dp), n,
+                                              C.byref(nnz)), self.engine.h)
+        return rows[:n], vals[:n], var[:n]
+
+    def result_dense(self, rid):
+        n = int(np.prod(self.engine.shape))
+        dose = np.zeros(n)
+        unc = np.zeros(n)
+        _check(lib().omc_server_result_dense(self.h, int(rid), _p(dose, _dp), _p(unc, _dp)), self.engine.h)
+        return dose.reshape(self.engine.shape), unc.reshape(self.engine.shape)
+
+    def release(self, rid):
+        _check(lib().omc_server_release(self.h, int(rid)), self.engine.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().omc_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def bixel_grid(phantom, gantry_deg, bixel=0.5, field=(5.0, 5.0), sad=100.0, iso=None):
+    """matRad-style beamlets of coplanar beams rotating about the z axis:
+    for each gantry angle a source point at distance `sad` from the
+    isocentre and a grid of `bixel`-sized squares (side1, side2) in the plane
+    through the isocentre perpendicular to the beam.  Returns the dict
+    accepted by Engine.run_beamlets / Server.beamlet_set."""
+    xb, yb, zb = phantom.xb, phantom.yb, phantom.zb
+    if iso is None:
+        iso = np.array([(xb[0] + xb[-1]) / 2, (yb[0] + yb[-1]) / 2, (zb[0] + zb[-1]) / 2])
+    src, corner, s1, s2, ibeam = [], [], [], [], []
+    nu = int(round(field[0] / bixel))
+    nv = int(round(field[1] / bixel))
+    for b, g in enumerate(gantry_deg):
+        t = np.deg2rad(g)
+        d = np.array([np.sin(t), -np.cos(t), 0.0])      # beam direction (source -> iso)
+        src.append(iso - sad * d)
+        e1 = np.array([np.cos(t), np.sin(t), 0.0]) * bixel
+        e2 = np.array([0.0, 0.0, 1.0]) * bixel
+        for i in range(nu):
+            for j in range(nv):
+                c = iso + (i - nu / 2) * e1 + (j - nv / 2) * e2
+                corner.append(c)
+                s1.append(e1)
+                s2.append(e2)
+                ibeam.append(b)
+    return dict(src=np.array(src), corner=np.array(corner), side1=np.array(s1), side2=np.array(s2),
+                ibeam=np.array(ibeam, dtype=np.int32))

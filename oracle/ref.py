@@ -172,6 +172,56 @@ class Reference:
         return ustep, used.value, fin
 
 
+MATRAD_LIB = REF_DIR / "libompmc_matrad_ref.so"
+_matrad = None
+
+
+def matrad_dij(phantom, beamlets, nhist, nbatch=10, seeds=(97, 33), ecut=0.7, pcut=0.01, rel_threshold=1e-4,
+               spectrum_file="", assets_root=None, gaussian=False, gauss_width=0.2123, cap=None):
+    """One call of the unmodified matRad MEX entry (omc_matrad.c:1417) through
+    the mex.h shim.  `beamlets` is the dict of ompmc_b200.engine.bixel_grid
+    (0-based ibeam).  Returns (colptr, rows, vals, var) of D and V."""
+    global _matrad
+    from ompmc_b200 import assets as A
+    root = Path(assets_root) if assets_root else A.require_assets()
+    if _matrad is None:
+        L = C.CDLL(str(MATRAD_LIB))
+        L.hm_dij.restype = C.c_long
+        L.hm_last_error.restype = C.c_char_p
+        _matrad = L
+    L = _matrad
+    nx, ny, nz = phantom.shape
+    rho = np.ascontiguousarray(phantom.rho, dtype=np.float64).ravel()
+    mat = np.ascontiguousarray(phantom.med, dtype=np.int32).ravel()
+    names = (C.c_char_p * len(phantom.media))(*[m.encode() for m in phantom.media])
+    xb, yb, zb = (np.ascontiguousarray(b, dtype=np.float64) for b in (phantom.xb, phantom.yb, phantom.zb))
+    ib = np.asarray(beamlets["ibeam"], dtype=np.float64) + 1.0
+    src = np.ascontiguousarray(beamlets["src"], dtype=np.float64)
+    cor = np.ascontiguousarray(beamlets["corner"], dtype=np.float64)
+    s1 = np.ascontiguousarray(beamlets["side1"], dtype=np.float64)
+    s2 = np.ascontiguousarray(beamlets["side2"], dtype=np.float64)
+    nbix, nbeams = len(cor), len(src)
+    cap = cap or max(1024, nx * ny * nz * nbix // 4)
+    jc = np.zeros(nbix + 1, dtype=np.int64)
+    ir = np.zeros(cap, dtype=np.int64)
+    pr = np.zeros(cap)
+    var = np.zeros(cap)
+    P = lambda a, t: a.ctypes.data_as(C.POINTER(t))
+    n = L.hm_dij(C.c_int(nx), C.c_int(ny), C.c_int(nz), P(rho, C.c_double), P(mat, C.c_int32),
+                 C.c_int(len(phantom.media)), names, P(xb, C.c_double), P(yb, C.c_double), P(zb, C.c_double),
+                 C.c_int(nbix), C.c_int(nbeams), P(ib, C.c_double), P(src, C.c_double), P(cor, C.c_double),
+                 P(s1, C.c_double), P(s2, C.c_double), C.c_double(nhist), C.c_double(nbatch),
+                 C.c_double(seeds[0]), C.c_double(seeds[1]), C.c_double(ecut), C.c_double(pcut),
+                 C.c_double(rel_threshold), str(spectrum_file).encode(),
+                 str(root / "pegs4" / "521icru.pegs4dat").encode(), str(root / "pegs4" / "pgs4form.dat").encode(),
+                 (str(root / "data") + "/").encode(), (str(root / "out") + "/").encode(), C.c_int(int(gaussian)),
+                 C.c_double(gauss_width), P(jc, C.c_long), P(ir, C.c_long), P(pr, C.c_double), P(var, C.c_double),
+                 C.c_long(cap))
+    if n < 0:
+        raise RuntimeError(f"matRad reference failed ({n}): {L.hm_last_error().decode(errors='replace')}")
+    return jc, ir[:n].copy(), pr[:n].copy(), var[:n].copy()
+
+
 def run_cli(inp_base, out_name, cores=None, timeout=3600):
     """Run the reference CLI on `<inp_base>.inp`; returns (seconds of the
     batch loop as the CLI reports it, path of the .3ddose).  `cores` pins

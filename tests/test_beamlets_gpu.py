@@ -1,0 +1,56 @@
+"""matRad D_ij parity: omc_run_beamlets against the unmodified matRad MEX
+entry (ucodes/omc_matrad/omc_matrad.c, run through the oracle's mex.h shim,
+tests/golden/dij_ctsmall.npz: 8 beamlets of 1x1 cm from gantry 0 and 90 deg
+on the 4-media CT-like phantom, 1e5 histories in 10 batches each).
+
+Per column, in voxels above 10 % of the reference column maximum,
+z = (D_gpu - D_ref) / sqrt(V_gpu + V_ref) with V the variance of the mean;
+|z| < 3 in >= 99 % and no bias.  The plain form reproduces the reference's
+variance accumulation across beamlets (omc_matrad.c:1702 never resets
+accum_endep2), so its test uses 2 V_ref; the event form's V is each
+beamlet's own.  Rows come out ascending and the column sizes above the
+1e-4 threshold match the reference's within noise."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def dij_inputs(golden):
+    g = golden("dij_ctsmall")
+    bl = dict(src=g["src"], corner=g["corner"], side1=g["side1"], side2=g["side2"], ibeam=g["ibeam"])
+    return g, bl
+
+
+def columns(colptr, rows, vals, var):
+    return [(rows[colptr[i]:colptr[i + 1]], vals[colptr[i]:colptr[i + 1]],
+             None if var is None else var[colptr[i]:colptr[i + 1]]) for i in range(len(colptr) - 1)]
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain_fp64", "event_fp32"])
+def test_dij_matches_matrad_reference(mode, golden, engine_for, assets_root):
+    from ompmc_b200.engine import load_spectrum
+    g, bl = dij_inputs(golden)
+    bl["spectrum"] = load_spectrum(assets_root / "spectra" / "6mv.spectrum")
+    eng = engine_for("ctsmall")
+    colptr, rows, vals, var, st = eng.run_beamlets(bl, int(g["nhist"]), int(g["nbatch"]), float(g["rel"]),
+                                                   seed=2024, mode=mode)
+    assert st["histories"] == 8 * int(g["nhist"])
+    ref = columns(g["colptr"], g["rows"], g["vals"], g["var"])
+    mine = columns(colptr, rows, vals, var)
+    zs = []
+    for i, ((rr, rv, rvar), (mr, mv, mvar)) in enumerate(zip(ref, mine)):
+        assert np.all(np.diff(mr) > 0), f"column {i}: rows not ascending"
+        nref = int(g["nnz_full"][i])
+        assert abs(len(mr) - nref) <= 0.15 * nref + 50, (i, len(mr), nref)
+        d = dict(zip(mr.tolist(), zip(mv.tolist(), mvar.tolist())))
+        sel = rv > 0.10 * rv.max()
+        for r, v, w in zip(rr[sel], rv[sel], rvar[sel]):
+            got, gv = d.get(int(r), (0.0, 0.0))
+            s2 = 2 * w if mode == 0 else gv + w
+            zs.append((got - v) / np.sqrt(s2))
+    zs = np.array(zs)
+    assert len(zs) > 300
+    frac = np.mean(np.abs(zs) < 3)
+    assert frac >= 0.99, f"|z|<3 in {frac:.4f}, mean z {zs.mean():.3f}"
+    assert abs(zs.mean()) < 0.25, zs.mean()
