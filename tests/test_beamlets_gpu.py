@@ -3,7 +3,7 @@ entry (ucodes/omc_matrad/omc_matrad.c, run through the oracle's mex.h shim,
 tests/golden/dij_ctsmall.npz: 8 beamlets of 1x1 cm from gantry 0 and 90 deg
 on the 4-media CT-like phantom, 1e5 histories in 10 batches each).
 
-Per column, in voxels above 10 % of the reference column maximum,
+Per column, in voxels above 5 % of the reference column maximum,
 z = (D_gpu - D_ref) / sqrt(V_gpu + V_ref) with V the variance of the mean;
 |z| < 3 in >= 99 % and no bias.  The plain form reproduces the reference's
 variance accumulation across beamlets (omc_matrad.c:1702 never resets
@@ -44,13 +44,13 @@ def test_dij_matches_matrad_reference(mode, golden, engine_for, assets_root):
         nref = int(g["nnz_full"][i])
         assert abs(len(mr) - nref) <= 0.15 * nref + 50, (i, len(mr), nref)
         d = dict(zip(mr.tolist(), zip(mv.tolist(), mvar.tolist())))
-        sel = rv > 0.10 * rv.max()
+        sel = rv > 0.05 * rv.max()
         for r, v, w in zip(rr[sel], rv[sel], rvar[sel]):
             got, gv = d.get(int(r), (0.0, 0.0))
             s2 = 2 * w if mode == 0 else gv + w
             zs.append((got - v) / np.sqrt(s2))
     zs = np.array(zs)
-    assert len(zs) > 300
+    assert len(zs) > 250
     frac = np.mean(np.abs(zs) < 3)
     assert frac >= 0.99, f"|z|<3 in {frac:.4f}, mean z {zs.mean():.3f}"
     assert abs(zs.mean()) < 0.25, zs.mean()
