@@ -170,6 +170,80 @@ def reference_rate(root, ph, spec_path, ncase, cores):
     return ncase / loop_s, loop_s
 
 
+GANTRY = [0.0, 51.0, 103.0, 154.0, 206.0, 257.0, 309.0]
+
+
+def bench_serving(device, nbeamlets, load=0.7, seed=7, plain_sample=12):
+    """beamlet dose-influence requests on the 128x128x96
+    x 0.3 cm CT-like phantom, 7 coplanar beams, 0.5x0.5 cm2 bixels at the
+    isocentre (SAD 100 cm), histories per beamlet log-uniform in
+    [2e4, 2e5], Poisson arrivals offered at `load` x measured capacity.
+    Returns latency percentiles and throughput of the served event form and
+    the plain FP64 form on a sample of the same beamlets (run one after the
+    other, as the reference does)."""
+    from ompmc_b200 import assets as A
+    from ompmc_b200.engine import PLAIN_FP64, Engine, Server, Tables, bixel_grid, load_spectrum
+    root = A.require_assets()
+    ph = A.ct_phantom(128, 128, 96, 0.3, seed=1234)
+    spec = load_spectrum(root / "spectra" / "6mv.spectrum")
+    eng = Engine(Tables.from_assets(A.CT_MEDIA, root), ph, device=device)
+    bl = bixel_grid(ph, GANTRY, bixel=0.5, field=(8.5, 8.5))        # 7 x 17 x 17 = 2023 bixels
+    bl["spectrum"] = spec
+    rng = np.random.default_rng(seed)
+    nb_all = len(bl["corner"])
+    pick = rng.choice(nb_all, size=min(nbeamlets, nb_all), replace=False)
+    nh = np.exp(rng.uniform(np.log(2e4), np.log(2e5), size=len(pick))).astype(np.int64) // 10 * 10
+    srv = Server(eng, seed=seed)
+    bs = srv.beamlet_set(bl)
+    # capacity probe: 16 requests back to back
+    t0 = time.perf_counter()
+    ids = [srv.submit_beamlet(bs, int(pick[i % len(pick)]), 50000, 10, 1e-4) for i in range(16)]
+    while srv.step(8) > 0:
+        pass
+    cap_hps = 16 * 50000 / (time.perf_counter() - t0)
+    for r in ids:
+        srv.release(r)
+    rate = load * cap_hps / float(nh.mean())                            # requests per second
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(pick)))
+    sub = {}
+    t_start = time.perf_counter()
+    k = 0
+    guard = 0
+    while True:
+        now = time.perf_counter() - t_start
+        while k < len(pick) and arrivals[k] <= now:
+            # the time between arrival and submission counts as latency
+            sub[k] = (srv.submit_beamlet(bs, int(pick[k]), int(nh[k]), 10, 1e-4), 1e3 * (now - arrivals[k]))
+            k += 1
+        active = srv.step(4)
+        if active == 0:
+            if k == len(pick):
+                break
+            time.sleep(max(0.0, min(0.002, arrivals[k] - (time.perf_counter() - t_start))))
+        guard += 1
+        if guard > 10_000_000:
+            raise RuntimeError("serving bench did not drain")
+    makespan = time.perf_counter() - t_start
+    lat = np.array([srv.poll(r) + lag for r, lag in sub.values()])
+    nnz = [len(srv.result_sparse(r)[0]) for r, _ in sub.values()]
+    srv.close()
+    served = float(nh.sum()) / makespan
+    # plain FP64 history-based form, beamlets one after the other
+    sample = {k: bl[k] for k in ("src", "corner", "side1", "side2", "ibeam")}
+    m = min(plain_sample, len(pick))
+    sample.update(corner=bl["corner"][pick[:m]], side1=bl["side1"][pick[:m]], side2=bl["side2"][pick[:m]],
+                  ibeam=bl["ibeam"][pick[:m]], spectrum=spec)
+    _, _, _, _, pst = eng.run_beamlets(sample, 50000, 10, 1e-4, seed=3, mode=PLAIN_FP64)
+    plain = pst["histories"] / pst["seconds"]
+    eng.close()
+    return {"workload": "ct128x128x96 x 0.3 cm, 7 coplanar beams, 0.5x0.5 cm2 bixels, log-uniform 2e4-2e5 "
+                        "histories, Poisson arrivals", "requests": len(pick), "histories": int(nh.sum()),
+            "offered_load_frac": load, "capacity_hist_per_s": cap_hps, "served_hist_per_s": served,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_nnz_per_column": float(np.mean(nnz)), "plain_fp64_hist_per_s": plain,
+            "speedup_served_vs_plain": served / plain}
+
+
 def host_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -221,6 +295,8 @@ def main():
     ap.add_argument("--hist-per-step", type=int, default=HIST_PER_STEP)
     ap.add_argument("--ref-sample", type=int, default=400_000)
     ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and plain comparator")
+    ap.add_argument("--serving-requests", type=int, default=300,
+                    help="beamlet requests in the serving workload (0 skips it)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -331,6 +407,8 @@ def main():
                                                     f"{s:.1f} s batch loop"}
             else:
                 extras["cpu_baseline"] = None
+        if args.serving_requests > 0 and world == 1:
+            extras["serving"] = bench_serving(local, args.serving_requests)
 
     if rank == 0:
         out = {

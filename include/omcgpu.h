@@ -103,6 +103,14 @@ const char *omc_engine_last_error(const omc_engine *e);
  * (deposits into one voxel in a row are summed first). */
 int omc_profile_last(const omc_engine *e, double *out, int n);
 
+/* Per-cycle trace of the last profiled event-form beam run: for cycle c,
+ * out[6c .. 6c+5] = histories injected, particles in the photon queue
+ * (injected primaries counted there) and in the electron queue at the start
+ * of the transport kernels, and the source, photon and electron kernel times
+ * in ms.  Copies at most max_cycles rows; returns the number of cycles
+ * of that run (0 when none was profiled). */
+int omc_profile_trace(const omc_engine *e, double *out, int max_cycles);
+
 /* ------------------------------------------------------------ sources */
 /* Energy distribution: a spectrum inverse CDF (cdf1/cdf2 of length n,
  * omc_dosxyz.c:474-494) or a mono-energetic source (n = 0). */

@@ -556,6 +556,16 @@ int omc_profile_last(const omc_engine *e, double *out, int n) {
     return OMC_OK;
 }
 
+int omc_profile_trace(const omc_engine *e, double *out, int max_cycles) {
+    if (!e || (max_cycles > 0 && !out)) return global_err(OMC_E_ARG, "omc_profile_trace: bad argument");
+    if (!e->ev) return 0;
+    const std::vector<double> &t = e->ev->trace;
+    int n = (int)(t.size() / 6);
+    int m = std::min(n, std::max(max_cycles, 0));
+    std::copy(t.begin(), t.begin() + (size_t)m * 6, out);
+    return n;
+}
+
 // ------------------------------------------------------------ beam runs
 int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, uint64_t seed, int mode, double *dose,
                  double *unc, double *stats) {

@@ -373,16 +373,26 @@ static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallie
                         long long target, Ctl &h, long &cycles) {
     EventState &S = *e->ev;
     for (auto &p : S.prof) p = KernelProfile();
+    S.trace.clear();
     cudaEvent_t ev[6];
     for (auto &x : ev) cudaEventCreate(&x);
     int rc = OMC_OK;
     cycles = 0;
+    int cnt_in[2] = {0, 0};   // queue sizes the cycle starts with (before injection)
     for (;;) {
-        launch_cycle(e, (int)(cycles & 1), src, tallies, nper, seed, target, ev);
+        int in = (int)(cycles & 1);
+        launch_cycle(e, in, src, tallies, nper, seed, target, ev);
         cycles++;
         if ((rc = cuda_check(e, cudaEventSynchronize(ev[5]), "profiled cycle"))) break;
         float t[5];
         for (int k = 0; k < 5; k++) cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]);
+        Ctl c;
+        cudaMemcpy(&c, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
+        int oph = in == 0 ? 2 : 0;
+        double row[6] = {(double)c.inject, (double)cnt_in[0] + c.inject, (double)cnt_in[1], t[1], t[2], t[3]};
+        S.trace.insert(S.trace.end(), row, row + 6);
+        cnt_in[0] = std::min(c.cnt[oph], S.cap);
+        cnt_in[1] = std::min(c.cnt[oph + 1], S.cap);
         S.prof[3].seconds += (t[0] + t[4]) * 1e-3;
         S.prof[3].launches += 2;
         S.prof[0].seconds += t[1] * 1e-3;

@@ -1,5 +1,6 @@
 // Event-based FP32 transport form (omc_event.cu).
 #pragma once
+#include <vector>
 #include "omc_engine.h"
 
 namespace omc {
@@ -48,6 +49,9 @@ struct EventState {
     int tsteps = 2;           // electron tstep iterations per event launch
     long long inflight = 0;   // particles kept in flight by the injector
     KernelProfile prof[4];    // 0 source, 1 photon, 2 electron, 3 plan+reset
+    // profiled runs: per cycle {histories injected, photons in, electrons in,
+    // source ms, photon ms, electron ms}
+    std::vector<double> trace;
 };
 
 // ------------------------------------------------------------ serving

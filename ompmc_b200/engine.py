@@ -5,9 +5,10 @@ Mirrors ompMC's two surfaces for the transport path:
 * `dosxyz(inp_base, out_name)` is the omc_dosxyz program
   (ucodes/omc_dosxyz/omc_dosxyz.c:1072-1307): same `.inp` keys, writes the
   same `.3ddose` file;
-* `matrad_dij(cubeRho, cubeMatIx, mcGeo, mcSrc, mcOpt)` is the matRad MEX
-  entry (ucodes/omc_matrad/omc_matrad.c:1417-1789): same inputs (dicts in
-  place of MATLAB structs), returns scipy CSC matrices D (and V).
+* `ompmc_b200.matrad.matrad_dij(cubeRho, cubeMatIx, mcGeo, mcSrc, mcOpt)`
+  is the matRad MEX entry (ucodes/omc_matrad/omc_matrad.c:1417-1789): same
+  inputs (dicts in place of MATLAB structs), returns scipy CSC matrices D
+  (and V); it runs on `Engine.run_beamlets` below.
 
 Errors raise `OmcError` carrying the library's status and message (the
 reference calls exit() or mexErrMsgIdAndTxt).  The library is loaded from the
@@ -99,6 +100,7 @@ def lib():
                               _lp, _ip, _dp, _dp, C.c_int64, _lp, _dp], C.c_int),
         "omc_dosxyz_run": ([C.c_char_p, C.c_char_p, C.c_int, C.c_int], C.c_int),
         "omc_profile_last": ([C.c_void_p, _dp, C.c_int], C.c_int),
+        "omc_profile_trace": ([C.c_void_p, _dp, C.c_int], C.c_int),
         "omc_run_beam_noalloc": ([C.c_void_p, C.POINTER(_Beam), C.c_int64, C.c_int, C.c_uint64, _dp, _dp, _dp],
                                  C.c_int),
         "omc_server_create": ([C.c_void_p, C.c_int64, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)], C.c_int),
@@ -334,6 +336,15 @@ class Engine:
         return {names[k]: dict(zip(keys, out[k * 7:(k + 1) * 7])) for k in range(4)}
 
     # ------------------------------------------------ validation hooks
+    def profile_trace(self):
+        """Per-cycle trace of the last profiled event-form run: array of rows
+        (injected, photons in, electrons in, source ms, photon ms, electron ms)."""
+        n = lib().omc_profile_trace(self.h, None, 0)
+        _check(min(n, 0), self.h)
+        out = np.zeros(max(n, 1) * 6)
+        lib().omc_profile_trace(self.h, _p(out, _dp), n)
+        return out[:n * 6].reshape(n, 6)
+
     def trace_rays(self, rays, cap=512):
         """FP64 device howfar walk per ray (x,y,z,u,v,w,ir)."""
         rays = np.ascontiguousarray(rays, dtype=np.float64)

@@ -125,6 +125,19 @@ int h_nvox(void) { return geometry.isize * geometry.jsize * geometry.ksize; }
 int h_nmed(void) { return media.nmed; }
 
 /* Reference tables by name, as flat arrays.  `n` receives the element count. */
+/* Leading members of omc_dosxyz.c's struct Source (omc_dosxyz.c:342-352),
+   declared here in the same order so the harness can read the inverse CDF
+   of the spectrum the reference built in initSource (omc_dosxyz.c:478-502). */
+struct SourceHead {
+    int spectrum;
+    int charge;
+    double energy;
+    double deltak;
+    double *cdfinv1;
+    double *cdfinv2;
+};
+extern struct SourceHead source;
+
 const void *h_table(const char *t, long *n) {
     int nmed = media.nmed;
 #define T(NAME, PTR, COUNT) if (strcmp(t, NAME) == 0) { *n = (COUNT); return (const void *)(PTR); }
@@ -175,6 +188,8 @@ const void *h_table(const char *t, long *n) {
     T("meke", pegs_data.meke, nmed)
     T("region_med", region.med, h_nvox() + 1) T("region_rhof", region.rhof, h_nvox() + 1)
     T("region_pcut", region.pcut, h_nvox() + 1) T("region_ecut", region.ecut, h_nvox() + 1)
+    T("cdfinv1", source.cdfinv1, source.spectrum ? (long)source.deltak : 0)
+    T("cdfinv2", source.cdfinv2, source.spectrum ? (long)source.deltak : 0)
 #undef T
     *n = 0;
     return NULL;
