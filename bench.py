@@ -1,11 +1,11 @@
 """Benchmark: histories/s of the event-based FP32-transport / FP64-tally form
 on the heterogeneous slab workload (64^3 voxels of 0.25 cm: water 0-3 cm,
 lung 3-8 cm, bone 8-10 cm, water; 5x5 cm^2 field of the 6 MV-like spectrum,
-10^7 histories = 10 steps of 10^6), one JSON line on stdout.
+10^7 histories per dose run), one JSON line on stdout.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-A step is one complete dose run of 10^6 histories in 10 batches through
+A step is one complete dose run of 10^7 histories in 10 batches through
 omc_run_beam (dose + batch uncertainty out).  `value` is device time of the
 transport (CUDA events on the engine's stream, tables/phantom resident);
 `e2e` times the same calls from the host with the spectrum upload and the
@@ -34,8 +34,8 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 METRIC = "histories/s at 1% dose unc. (served vs plain GPU vs CPU); p50/p99 beamlet ms"
-WORKLOAD = "slab64: 64^3 x 0.25 cm water/lung(0.26)/bone(1.85)/water, 5x5 cm2 6MV-like, 1e6 histories x 10 batches per step"
-HIST_PER_STEP = 1_000_000
+WORKLOAD = "slab64: 64^3 x 0.25 cm water/lung(0.26)/bone(1.85)/water, 5x5 cm2 6MV-like, 1e7 histories in 10 batches per step"
+HIST_PER_STEP = 10_000_000
 NBATCH = 10
 COLLIMATOR = (-2.5, 2.5, -2.5, 2.5)
 MEDIA = ["H2O521ICRU", "LUNG521ICRU", "ICRPBONE521ICRU"]
@@ -293,10 +293,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="event", choices=["event", "plain"])
     ap.add_argument("--hist-per-step", type=int, default=HIST_PER_STEP)
-    ap.add_argument("--ref-sample", type=int, default=400_000)
+    ap.add_argument("--ref-sample", type=int, default=10_000_000)
     ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and plain comparator")
     ap.add_argument("--serving-requests", type=int, default=300,
                     help="beamlet requests in the serving workload (0 skips it)")
+    ap.add_argument("--cycle-trace", action="store_true",
+                    help="print the per-cycle trace (queue sizes, kernel ms) of the first warm-up step and exit")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -323,6 +325,17 @@ def main():
     def step(i, e=eng, m=mode, n=nstep):
         return e.run_beam(n, NBATCH, seed=seed0 + i, mode=m, spectrum=spec, collimator=COLLIMATOR)
 
+    if args.cycle_trace:
+        # same seed as the first warm-up step: the queue sizes per cycle are
+        # those of the launches a profiler sees first
+        te = Engine(tables, ph, ecut=0.7, pcut=0.01, device=local, profile=True)
+        te.run_beam(nstep, NBATCH, seed=seed0 - 1, mode=EVENT_FP32, spectrum=spec, collimator=COLLIMATOR)
+        rows = te.profile_trace()
+        te.close()
+        cols = ["injected", "photons", "electrons", "source_ms", "photon_ms", "electron_ms"]
+        print(json.dumps({"seed": seed0 - 1, "histories": nstep, "columns": cols, "cycles": rows.tolist()}))
+        eng.close()
+        return 0
     for i in range(args.warmup):
         step(-1 - i)
     sampler = ClockSampler(local)
@@ -373,6 +386,10 @@ def main():
             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
             "traffic": (tpe * per_launch_events) if tpe else None,
             "algorithmic_bytes_per_launch": alg_bytes / max(1, ek["launches"]),
+            # particle-state queue traffic, reported apart from the algorithmic
+            # figure: 52 B loaded and 52 B stored per electron event
+            "state_bytes_per_launch": 104 * per_launch_events,
+            "achieved_with_state": (alg_bytes + 104 * ek["particles"]) / ek["seconds"] / 1e9,
             "avg_launch_ms": 1000 * ek["seconds"] / max(1, ek["launches"]),
             "kernel_share": {k: v["seconds"] for k, v in prof.items()},
         }
@@ -392,7 +409,7 @@ def main():
                               "seconds_to_1pct": nstep * (unc1 / 0.01) ** 2 / value}
         if not args.no_extras and world == 1:
             # plain FP64 history-based form on the same workload (comparator)
-            pn = max(nstep // 2, 100000)
+            pn = max(nstep // 5, 100000)
             step(999, m=PLAIN_FP64, n=pn)
             _, _, pst = step(1000, m=PLAIN_FP64, n=pn)
             plain = pn / pst["seconds"]

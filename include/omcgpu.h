@@ -84,6 +84,9 @@ typedef struct {
     int electron_tsteps;  /* event form: tstep-loop iterations an electron runs
                              per launch before it is re-queued (0 = default) */
     int64_t inflight;     /* event form: particles kept in flight (0 = default) */
+    int tail_boost;       /* event form: largest factor by which event budgets
+                             grow as the queues drain (0 = default 32, 1 = fixed
+                             budgets); results do not depend on it */
 } omc_options;
 
 void omc_options_default(omc_options *o);
@@ -96,7 +99,7 @@ const char *omc_engine_last_error(const omc_engine *e);
 
 /* Per-kernel profile of the last event-form omc_run_beam made with
  * options.profile = 1.  out (n >= 28) receives, for kernel k = 0 source,
- * 1 photon transport, 2 electron transport, 3 plan + reset, the values
+ * 1 photon transport, 2 electron transport, 3 cycle planning, the values
  * out[k*7 + j]: j = 0 launches, 1 device seconds, 2 particles processed,
  * 3 transport steps (photon voxel steps, electron CH/BCA steps),
  * 4 voxel-boundary crossings, 5 energy deposits, 6 FP64 tally atomics

@@ -11,6 +11,17 @@ namespace omc {
 #ifndef OMC_HD
 #define OMC_HD __host__ __device__ __forceinline__
 #endif
+#ifndef OMC_COLD
+// Interaction samplers and other code that runs at most once per event:
+// one out-of-line copy keeps the transport kernels small enough for the
+// instruction caches.
+#define OMC_COLD __host__ __device__ __noinline__
+#endif
+#ifndef OMC_OUTLINE
+// Large routines called from several sites of the electron step (one copy
+// instead of one per call site, for the same reason).
+#define OMC_OUTLINE __host__ __device__ __noinline__
+#endif
 
 constexpr int D_MXGE = 2000;
 constexpr int D_MXEKE = 500;

@@ -1,18 +1,25 @@
 // Event-based FP32 transport: structure-of-arrays particle queues, one
-// transport event (one call of ompMC's photon() or electron(), until the next
-// interaction or death) per thread per launch, outputs appended with
+// transport event per queued particle per launch, outputs appended with
 // warp-aggregated atomics, FP64 tallies per batch slot.
 //
-// A transport cycle is five launches on one stream:
-//   k_plan      how many new histories fit (in-flight target - occupancy)
+// A transport cycle is four launches on one stream:
+//   k_plan      how many new histories fit (in-flight target - occupancy),
+//               the electron budget of this cycle, output queues emptied
 //   k_source    primaries of those histories into the input queues
 //   k_photon    one photon event per queued photon
 //   k_electron  one electron event per queued e-/e+
-//   k_reset     input queues consumed
 // Queues are double-buffered (A -> B, then B -> A), so two cycles form an
 // idempotent CUDA graph that the host replays until every history is done.
-// Each particle carries its own Philox stream (key, block counter), so the
-// result does not depend on scheduling.
+//
+// An event transports its particle until the next interaction, death or,
+// for electrons, the end of the cycle's budget of tstep-loop iterations.
+// The budget is small while the queues fill the GPU (lanes of a warp then do
+// similar work) and grows as they drain, so the drain tail takes few
+// cycles.  Each particle carries its own Philox stream (key, position) and
+// secondaries get keys from the parent's key and stream position at their
+// creation, so a particle's trajectory does not depend on where events are
+// cut nor on scheduling: any budget gives the same result up to the
+// summation order of the FP64 tallies.
 #include <algorithm>
 #include <cstdio>
 
@@ -23,7 +30,7 @@
 namespace omc {
 
 constexpr int EV_BUDGET = 200000;  // transport steps one event may take
-constexpr int EV_MAXOUT = 3;       // particles an event may emit
+constexpr int EV_MAXOUT = 1;       // secondaries an event emits: every interaction sampler pushes one
 
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
@@ -37,9 +44,11 @@ struct EvEnv {
     int pend_ir;
     double pend_e;
     Part<float> out[EV_MAXOUT];
+    uint32_t out_pos[EV_MAXOUT];  // parent's stream position at each push
     int nout;
     unsigned flags;
     int work;
+    int tleft;                    // tstep-loop iterations left in this event
     int ncross, ndep, natom;
     __device__ float uni() { return rng.uni(); }
     // Consecutive deposits into one voxel are summed before the atomic.
@@ -60,13 +69,13 @@ struct EvEnv {
         pend_ir = -1;
     }
     __device__ void cross() { ncross++; }
-    int tsteps;
-    __device__ int tstep_budget() const { return tsteps; }
+    __device__ bool tstep_take() { return tleft-- > 0; }
     __device__ bool push(const Part<float> &q) {
         if (nout >= EV_MAXOUT) {
             flags |= ERR_STACK;
             return false;
         }
+        out_pos[nout] = rng.position();
         out[nout++] = q;
         return true;
     }
@@ -119,50 +128,42 @@ __device__ __forceinline__ int warp_append(const Queue &q, bool want, unsigned a
     return idx;
 }
 
-__device__ __forceinline__ void renorm(Part<float> &p) {
-    float n2 = p.u * p.u + p.v * p.v + p.w * p.w;
-    if (n2 > 0.f && fabsf(n2 - 1.f) > 1e-6f) {
-        float r = rsqrtf(n2);
-        p.u *= r; p.v *= r; p.w *= r;
-    }
-}
-
 // Route the event's surviving particle and its secondaries to the output
-// queues.  Secondaries get fresh streams derived from the parent's key and
-// block counter, which is unique per event.  Returns the particles queued.
-__device__ __forceinline__ int emit(const Queue &outP, const Queue &outE, unsigned active, bool alive,
-                                    Part<float> &p, EvEnv &g, int slot, uint32_t k0, uint32_t k1) {
+// queues.  A secondary's stream key is derived from its parent's key and
+// the parent's stream position when it was created.  All 32 lanes of the
+// warp take part (lanes without a particle pass alive = false, nout = 0).
+// Returns the particles this lane queued.
+__device__ __forceinline__ int emit(const Queue &outP, const Queue &outE, bool alive, const Part<float> &p,
+                                    EvEnv &g, int slot, uint32_t k0, uint32_t k1) {
+    const unsigned full = 0xffffffffu;
     uint64_t pkey = ((uint64_t)k1 << 32) | k0;
-    uint32_t pctr = g.rng.ctr;
     int queued = 0;
 #pragma unroll
     for (int k = 0; k < 1 + EV_MAXOUT; k++) {
         bool has;
         Part<float> q;
+        uint32_t a0 = k0, a1 = k1, ac;
         if (k == 0) {
             has = alive;
             q = p;
+            ac = g.rng.position();
         } else {
             has = k - 1 < g.nout;
-            q = g.out[k - 1 < EV_MAXOUT ? k - 1 : 0];
+            q = g.out[k - 1];
+            uint64_t ck = mix64(pkey * 0x9E3779B97F4A7C15ull + ((uint64_t)g.out_pos[k - 1] << 1) + 1u);
+            a0 = (uint32_t)ck;
+            a1 = (uint32_t)(ck >> 32);
+            ac = 0;
         }
-        if (__ballot_sync(active, has) == 0) continue;
-        if (has) renorm(q);
+        if (__ballot_sync(full, has) == 0) continue;
         if (has && !(q.e == q.e && q.x == q.x && q.u == q.u)) {
             g.flags |= ERR_NAN;
             has = false;
         }
         bool isph = has && q.iq == 0;
         bool isel = has && q.iq != 0;
-        int ip = warp_append(outP, isph, active, g.flags);
-        int ie = warp_append(outE, isel, active, g.flags);
-        uint32_t a0 = k0, a1 = k1, ac = pctr;
-        if (k > 0) {
-            uint64_t ck = mix64(pkey * 0x9E3779B97F4A7C15ull + ((uint64_t)pctr << 3) + (uint64_t)k);
-            a0 = (uint32_t)ck;
-            a1 = (uint32_t)(ck >> 32);
-            ac = 0;
-        }
+        int ip = warp_append(outP, isph, full, g.flags);
+        int ie = warp_append(outE, isel, full, g.flags);
         if (ip >= 0) qstore(outP, ip, q, slot, a0, a1, ac);
         if (ie >= 0) qstore(outE, ie, q, slot, a0, a1, ac);
         queued += (ip >= 0) + (ie >= 0);
@@ -190,68 +191,78 @@ __device__ __forceinline__ void add_live(int *live, int nbmax, int slot, int del
     if (tot != 0 && (threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&live[req], tot);
 }
 
+// Events of one queue.  Warps take 32 particles at a time from a counter,
+// so work is balanced between warps however long their events run.
 template <bool PHOTON>
 __device__ __forceinline__ void transport_events(const DevData<float> &D, const Queue &in, const Queue &outP,
                                                  const Queue &outE, double *tallies, long nvox, Ctl *ctl,
-                                                 uint32_t seedw, int tsteps, int *live, int nbmax) {
-    int n = min(*in.count, in.cap);
+                                                 uint32_t seedw, int *live, int nbmax) {
+    const unsigned full = 0xffffffffu;
+    const int kq = PHOTON ? 0 : 1;
+    const int n = min(*in.count, in.cap);
+    const int tsteps = ctl->tsteps;
+    const int lane = threadIdx.x & 31;
     unsigned flags = 0;
     unsigned c_ev = 0, c_steps = 0, c_cross = 0, c_dep = 0, c_atom = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        unsigned active = __activemask();
+    for (int guard = 0; guard < (1 << 26); guard++) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&ctl->fetch[kq], 32);
+        base = __shfl_sync(full, base, 0);
+        if (base >= n) break;
+        const int i = base + lane;
+        const bool valid = i < n;
         Part<float> p;
-        int tag;
-        uint32_t k0, k1, ctr;
-        qload(in, i, p, tag, k0, k1, ctr);
-        int slot = tag >> 2;
+        int tag = 0;
+        uint32_t k0 = 0, k1 = 0, pos = 0;
+        if (valid) qload(in, i, p, tag, k0, k1, pos);
+        const int slot = tag >> 2;
         EvEnv g;
-        g.rng.init(((uint64_t)k1 << 32) | k0, seedw, ctr);
+        g.rng.init(((uint64_t)k1 << 32) | k0, seedw, pos);
         g.tally = tallies + (long)slot * nvox;
         g.pend_ir = -1;
         g.pend_e = 0.0;
         g.nout = 0;
         g.flags = 0;
         g.work = 0;
-        g.tsteps = tsteps;
+        g.tleft = tsteps;
         g.ncross = g.ndep = g.natom = 0;
-        bool alive;
-        if (PHOTON) alive = photon_step(D, g, p);
-        else alive = electron_step(D, g, p) == E_ALIVE;
-        g.flush();
-        int emitted = emit(outP, outE, active, alive, p, g, slot, k0, k1);
-        if (live) add_live(live, nbmax, slot, emitted - 1, active);
+        bool alive = false;
+        if (valid) {
+            alive = PHOTON ? photon_step(D, g, p) : electron_step(D, g, p) == E_ALIVE;
+            g.flush();
+        }
+        int emitted = emit(outP, outE, alive, p, g, slot, k0, k1);
+        if (live) add_live(live, nbmax, valid ? slot : 0, valid ? emitted - 1 : 0, full);
         flags |= g.flags;
-        c_ev++;
+        c_ev += valid;
         c_steps += g.work;
         c_cross += g.ncross;
         c_dep += g.ndep;
         c_atom += g.natom;
     }
-    unsigned active = __activemask();
-    report_flags(ctl, flags, active);
-    const int k = PHOTON ? 0 : 1;
-    report_count(&ctl->st_events[k], c_ev, active);
-    report_count(&ctl->st_steps[k], c_steps, active);
-    report_count(&ctl->st_cross[k], c_cross, active);
-    report_count(&ctl->st_dep[k], c_dep, active);
-    report_count(&ctl->st_atom[k], c_atom, active);
+    report_flags(ctl, flags, full);
+    report_count(&ctl->st_events[kq], c_ev, full);
+    report_count(&ctl->st_steps[kq], c_steps, full);
+    report_count(&ctl->st_cross[kq], c_cross, full);
+    report_count(&ctl->st_dep[kq], c_dep, full);
+    report_count(&ctl->st_atom[kq], c_atom, full);
 }
 
-// One photon event per queued photon.  `live` (may be null) receives the
+// Photon events of the queued photons.  `live` (may be null) receives the
 // change of each serving request's live-particle count.
 __global__ void __launch_bounds__(256) k_photon_step(DevData<float> D, Queue in, Queue outP, Queue outE,
                                                      double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
                                                      int *live, int nbmax) {
-    transport_events<true>(D, in, outP, outE, tallies, nvox, ctl, seedw, 1 << 30, live, nbmax);
+    transport_events<true>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax);
 }
 
-// One bounded electron/positron event per queued charged particle: at most
-// `tsteps` iterations of electron()'s tstep loop, then the particle is
-// re-queued, so every lane of a warp does a similar amount of work.
+// Electron/positron events of the queued charged particles: at most the
+// cycle's budget of tstep-loop iterations each, then the particle is
+// re-queued.
 __global__ void __launch_bounds__(256) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
                                                        double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
-                                                       int tsteps, int *live, int nbmax) {
-    transport_events<false>(D, in, outP, outE, tallies, nvox, ctl, seedw, tsteps, live, nbmax);
+                                                       int *live, int nbmax) {
+    transport_events<false>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax);
 }
 
 __global__ void k_source(DevData<float> D, BeamSrc<float> S, Queue qP, Queue qE, Ctl *ctl, long long nper,
@@ -272,8 +283,8 @@ __global__ void k_source(DevData<float> D, BeamSrc<float> S, Queue qP, Queue qE,
         int slot = (int)(h / nper);
         int ip = warp_append(qP, p.iq == 0, active, flags);
         int ie = warp_append(qE, p.iq != 0, active, flags);
-        if (ip >= 0) qstore(qP, ip, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.ctr);
-        if (ie >= 0) qstore(qE, ie, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.ctr);
+        if (ip >= 0) qstore(qP, ip, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.position());
+        if (ie >= 0) qstore(qE, ie, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.position());
     }
     for (int o = 16; o > 0; o >>= 1) es += __shfl_down_sync(0xffffffffu, es, o);
     if ((threadIdx.x & 31) == 0 && es != 0.0) atomicAdd(&ctl->src_energy, es);
@@ -281,23 +292,39 @@ __global__ void k_source(DevData<float> D, BeamSrc<float> S, Queue qP, Queue qE,
     report_flags(ctl, flags, active);
 }
 
-// Histories to inject this cycle: keep `target` particles in flight.
-__global__ void k_plan(Ctl *ctl, int iph, int iel, long long target, int cap) {
-    long long occ = (long long)min(ctl->cnt[iph], cap) + min(ctl->cnt[iel], cap);
+// Electron budget of a cycle whose electron queue holds nE particles on a
+// GPU with `lanes` resident threads: the base budget while the queue fills
+// the GPU, multiplied by up to `boost` as it drains (the drain tail then
+// takes few cycles; a lane's events of any length give the same result).
+__device__ __forceinline__ void plan_budget(Ctl *ctl, long long nE, const PlanCfg &c) {
+    long long me = 1;
+    if (c.boost > 1 && nE < c.lanes) {
+        me = c.lanes / (nE > 0 ? nE : 1);
+        me = me > c.boost ? c.boost : me;
+    }
+    ctl->tsteps = (int)(c.tsteps * me);
+    ctl->fetch[0] = 0;
+    ctl->fetch[1] = 0;
+}
+
+// Histories to inject this cycle: keep `target` particles in flight.  Also
+// sets the cycle's electron budget and empties the output queues (the
+// previous cycle's inputs, all consumed).
+__global__ void k_plan(Ctl *ctl, int iph, int iel, PlanCfg c) {
+    int oph = iph ^ 2, oel = iel ^ 2;
+    long long np = min(ctl->cnt[iph], c.cap), ne = min(ctl->cnt[iel], c.cap);
     long long rem = ctl->hist_total - ctl->hist_next;
-    long long inj = target - occ;
+    long long inj = c.target - (np + ne);
     if (inj < 0) inj = 0;
     if (inj > rem) inj = rem;
-    long long room = (long long)cap - ctl->cnt[iph];
+    long long room = (long long)c.cap - ctl->cnt[iph];
     if (inj > room) inj = room > 0 ? room : 0;
     ctl->inject = (int)inj;
     ctl->hist_base = ctl->hist_next;
     ctl->hist_next += inj;
-}
-
-__global__ void k_reset(Ctl *ctl, int iph, int iel) {
-    ctl->cnt[iph] = 0;
-    ctl->cnt[iel] = 0;
+    ctl->cnt[oph] = 0;
+    ctl->cnt[oel] = 0;
+    plan_budget(ctl, ne, c);
 }
 
 // ------------------------------------------------------------------ host
@@ -324,10 +351,18 @@ int event_prepare(omc_engine *e) {
     EventState &S = *e->ev;
     long cap = e->opt.queue_capacity > 0 ? e->opt.queue_capacity : (1L << 22);
     S.cap = (int)std::min(cap, (long)(1L << 30));
-    S.block = e->opt.block > 0 ? e->opt.block : 256;
-    S.grid = e->sm_count * (2048 / S.block);
-    // 2 measured best on the slab workload (sweep of 1..16 on a B200)
+    // warps fetch work 32 particles at a time: whole warps per block
+    S.block = e->opt.block > 0 ? std::min(1024, (e->opt.block + 31) / 32 * 32) : 256;
+    S.grid = e->sm_count * std::max(1, 2048 / S.block);
+    int bp = 0, be = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_photon_step, S.block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, k_electron_step, S.block, 0);
+    S.grid_p = e->sm_count * std::max(1, bp);
+    S.grid_e = e->sm_count * std::max(1, be);
+    S.lanes = S.grid_e * S.block;
+    // 2 measured best on the slab workload while the queues are full
     S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 2;
+    S.boost = e->opt.tail_boost > 0 ? e->opt.tail_boost : 32;
     S.inflight = e->opt.inflight > 0 ? e->opt.inflight : (1LL << 20);
     int rc = S.ctl.alloc(sizeof(Ctl));
     if (rc) return set_err(e, rc, "control block allocation failed");
@@ -336,6 +371,17 @@ int event_prepare(omc_engine *e) {
         if ((rc = alloc_queue(e, S.buf[i], S.q[i], S.cap, &S.ctl_d->cnt[i]))) return rc;
     S.ready = true;
     return OMC_OK;
+}
+
+PlanCfg plan_cfg(const omc_engine *e, long long target) {
+    const EventState &S = *e->ev;
+    PlanCfg c;
+    c.target = target;
+    c.cap = S.cap;
+    c.lanes = S.lanes;
+    c.boost = S.boost;
+    c.tsteps = S.tsteps;
+    return c;
 }
 
 void event_release(omc_engine *e) {
@@ -353,28 +399,27 @@ static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, doubl
     uint32_t seedw = (uint32_t)(seed >> 32);
     long nvox = e->ph.nvox();
     if (ev) cudaEventRecord(ev[0], e->stream);
-    k_plan<<<1, 1, 0, e->stream>>>(S.ctl_d, iph, iel, target, S.cap);
+    k_plan<<<1, 1, 0, e->stream>>>(S.ctl_d, iph, iel, plan_cfg(e, target));
     if (ev) cudaEventRecord(ev[1], e->stream);
     k_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, src, S.q[iph], S.q[iel], S.ctl_d, nper, seed, seedw);
     if (ev) cudaEventRecord(ev[2], e->stream);
-    k_photon_step<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
-                                                          S.ctl_d, seedw, nullptr, 1);
+    k_photon_step<<<S.grid_p, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
+                                                            S.ctl_d, seedw, nullptr, 1);
     if (ev) cudaEventRecord(ev[3], e->stream);
-    k_electron_step<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
-                                                           S.ctl_d, seedw, S.tsteps, nullptr, 1);
+    k_electron_step<<<S.grid_e, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
+                                                             S.ctl_d, seedw, nullptr, 1);
     if (ev) cudaEventRecord(ev[4], e->stream);
-    k_reset<<<1, 1, 0, e->stream>>>(S.ctl_d, iph, iel);
-    if (ev) cudaEventRecord(ev[5], e->stream);
 }
 
 // Profiled transport: cycles launched one by one with events around each
-// kernel; per-kernel device time accumulated into S.prof.
+// kernel; per-kernel device time accumulated into S.prof, one trace row per
+// cycle.
 static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallies, long nper, uint64_t seed,
                         long long target, Ctl &h, long &cycles) {
     EventState &S = *e->ev;
     for (auto &p : S.prof) p = KernelProfile();
     S.trace.clear();
-    cudaEvent_t ev[6];
+    cudaEvent_t ev[5];
     for (auto &x : ev) cudaEventCreate(&x);
     int rc = OMC_OK;
     cycles = 0;
@@ -383,29 +428,25 @@ static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallie
         int in = (int)(cycles & 1);
         launch_cycle(e, in, src, tallies, nper, seed, target, ev);
         cycles++;
-        if ((rc = cuda_check(e, cudaEventSynchronize(ev[5]), "profiled cycle"))) break;
-        float t[5];
-        for (int k = 0; k < 5; k++) cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]);
-        Ctl c;
-        cudaMemcpy(&c, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
+        if ((rc = cuda_check(e, cudaEventSynchronize(ev[4]), "profiled cycle"))) break;
+        float t[4];
+        for (int k = 0; k < 4; k++) cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]);
+        cudaMemcpy(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
         int oph = in == 0 ? 2 : 0;
-        double row[6] = {(double)c.inject, (double)cnt_in[0] + c.inject, (double)cnt_in[1], t[1], t[2], t[3]};
+        double row[6] = {(double)h.inject, (double)cnt_in[0] + h.inject, (double)cnt_in[1], t[1], t[2], t[3]};
         S.trace.insert(S.trace.end(), row, row + 6);
-        cnt_in[0] = std::min(c.cnt[oph], S.cap);
-        cnt_in[1] = std::min(c.cnt[oph + 1], S.cap);
-        S.prof[3].seconds += (t[0] + t[4]) * 1e-3;
-        S.prof[3].launches += 2;
+        cnt_in[0] = std::min(h.cnt[oph], S.cap);
+        cnt_in[1] = std::min(h.cnt[oph + 1], S.cap);
+        S.prof[3].seconds += t[0] * 1e-3;
+        S.prof[3].launches += 1;
         S.prof[0].seconds += t[1] * 1e-3;
         S.prof[0].launches += 1;
         S.prof[1].seconds += t[2] * 1e-3;
         S.prof[1].launches += 1;
         S.prof[2].seconds += t[3] * 1e-3;
         S.prof[2].launches += 1;
-        if ((cycles & 1) == 0) {
-            cudaMemcpy(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
-            if (h.hist_next >= h.hist_total && h.cnt[0] == 0 && h.cnt[1] == 0) break;
-            if (h.flags & ERR_QUEUE) break;
-        }
+        if (h.hist_next >= h.hist_total && cnt_in[0] == 0 && cnt_in[1] == 0) break;
+        if (h.flags & ERR_QUEUE) break;
         if (cycles > 200000) {
             rc = set_err(e, OMC_E_DEVICE, "event transport did not drain");
             break;
@@ -456,7 +497,7 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
         cudaEventDestroy(t0);
         cudaEventDestroy(t1);
         ks.seconds = ms * 1e-3;
-        ks.launches = cycles * 5 + nbatch;
+        ks.launches = cycles * 4 + nbatch;
         ks.flags |= h.flags;
         for (int k = 0; k < 2; k++) {
             KernelProfile &P = S.prof[1 + k];
@@ -495,7 +536,8 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
         graphs += per_check;
         cudaMemcpyAsync(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost, e->stream);
         if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "event transport"))) break;
-        if (h.hist_next >= h.hist_total && h.cnt[0] == 0 && h.cnt[1] == 0 && h.cnt[2] == 0 && h.cnt[3] == 0) break;
+        // a graph ends with a B -> A cycle: its outputs are queues A
+        if (h.hist_next >= h.hist_total && h.cnt[0] == 0 && h.cnt[1] == 0) break;
         if (h.flags & ERR_QUEUE) break;
         // every cycle advances each queued particle by one event, so a run
         // needs (histories / injection rate) + (longest history) cycles
@@ -513,7 +555,7 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
     float ms = 0;
     cudaEventElapsedTime(&ms, t0, t1);
     ks.seconds = ms * 1e-3;
-    ks.launches = graphs * 10 + nbatch;
+    ks.launches = graphs * 8 + nbatch;
     ks.flags |= h.flags;
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
@@ -528,12 +570,13 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
 // ============================================================== serving
 // Histories to inject this cycle across the admitted requests, first come
 // first served, keeping `target` particles in flight.
-__global__ void k_serve_plan(ServeDev *sd, Ctl *ctl, int iph, int iel, long long target, int cap) {
-    long long occ = (long long)min(ctl->cnt[iph], cap) + min(ctl->cnt[iel], cap);
-    long long room = target - occ;
+__global__ void k_serve_plan(ServeDev *sd, Ctl *ctl, int iph, int iel, PlanCfg c) {
+    const int cap = c.cap;
+    long long np = min(ctl->cnt[iph], cap), ne = min(ctl->cnt[iel], cap);
+    long long room = c.target - (np + ne);
     long long qroom = (long long)cap - max(ctl->cnt[iph], ctl->cnt[iel]);
     if (room > qroom) room = qroom;
-    int np = 0;
+    int nplan = 0;
     long long cum = 0;
     for (int k = 0; k < sd->norder && room - cum > 0; k++) {
         int s = sd->order[k];
@@ -542,16 +585,19 @@ __global__ void k_serve_plan(ServeDev *sd, Ctl *ctl, int iph, int iel, long long
         long long rem = r.nhist - r.next;
         if (rem <= 0) continue;
         long long take = rem < room - cum ? rem : room - cum;
-        sd->plan_slot[np] = s;
-        sd->plan_first[np] = r.next;
-        sd->plan_cum[np] = (int)cum;
+        sd->plan_slot[nplan] = s;
+        sd->plan_first[nplan] = r.next;
+        sd->plan_cum[nplan] = (int)cum;
         cum += take;
         r.next += take;
-        np++;
+        nplan++;
     }
-    sd->plan_cum[np] = (int)cum;
-    sd->nplan = np;
+    sd->plan_cum[nplan] = (int)cum;
+    sd->nplan = nplan;
     sd->inject_total = (int)cum;
+    ctl->cnt[iph ^ 2] = 0;
+    ctl->cnt[iel ^ 2] = 0;
+    plan_budget(ctl, ne, c);
 }
 
 // Primaries of the planned histories; each history's stream key is derived
@@ -579,8 +625,8 @@ __global__ void k_serve_source(DevData<float> D, ServeDev *sd, Queue qP, Queue q
         int slot = s * nbmax + (int)(local / r.nper);
         int ip = warp_append(qP, p.iq == 0, active, flags);
         int ie = warp_append(qE, p.iq != 0, active, flags);
-        if (ip >= 0) qstore(qP, ip, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.ctr);
-        if (ie >= 0) qstore(qE, ie, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.ctr);
+        if (ip >= 0) qstore(qP, ip, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.position());
+        if (ie >= 0) qstore(qE, ie, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.position());
         add_live(sd->live, nbmax, slot, (ip >= 0) + (ie >= 0), active);
     }
     unsigned active = __activemask();
@@ -593,13 +639,12 @@ void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, in
     int oph = in == 0 ? 2 : 0, oel = oph + 1;
     uint32_t seedw = 0x5e7e5eedu;
     long nvox = e->ph.nvox();
-    k_serve_plan<<<1, 1, 0, e->stream>>>(sd, S.ctl_d, iph, iel, target, S.cap);
+    k_serve_plan<<<1, 1, 0, e->stream>>>(sd, S.ctl_d, iph, iel, plan_cfg(e, target));
     k_serve_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, sd, S.q[iph], S.q[iel], S.ctl_d, nbmax, seedw);
-    k_photon_step<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox, S.ctl_d,
-                                                      seedw, sd->live, nbmax);
-    k_electron_step<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
-                                                        S.ctl_d, seedw, S.tsteps, sd->live, nbmax);
-    k_reset<<<1, 1, 0, e->stream>>>(S.ctl_d, iph, iel);
+    k_photon_step<<<S.grid_p, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
+                                                        S.ctl_d, seedw, sd->live, nbmax);
+    k_electron_step<<<S.grid_e, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
+                                                          S.ctl_d, seedw, sd->live, nbmax);
 }
 
 }  // namespace omc

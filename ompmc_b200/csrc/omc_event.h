@@ -7,7 +7,7 @@ namespace omc {
 
 // Structure-of-arrays particle queue in device memory.  `tag` packs the
 // charge (iq+1, 2 bits) and the tally slot (upper bits); k0/k1 are the
-// particle's Philox stream key and ctr its block counter.
+// particle's Philox stream key and ctr its stream position (numbers drawn).
 struct Queue {
     float *x, *y, *z, *u, *v, *w, *e, *wt;
     int *ir, *tag;
@@ -27,7 +27,9 @@ struct Ctl {
     unsigned flags;           // DevErr bits
     int pad;
     double src_energy;        // sum of primary kinetic energies
-    double edep;              // unused
+    int tsteps;               // this cycle's electron budget (tstep-loop iterations per event)
+    int pad2;
+    int fetch[2];             // work counters of the photon and electron kernels
     // counters per transport kernel (0 photon, 1 electron)
     unsigned long long st_events[2], st_steps[2], st_cross[2], st_dep[2], st_atom[2];
 };
@@ -35,6 +37,15 @@ struct Ctl {
 // Per-kernel profile of the last run made with options.profile = 1.
 struct KernelProfile {
     double launches = 0, seconds = 0, particles = 0, steps = 0, cross = 0, dep = 0, atom = 0;
+};
+
+// Per-cycle planning parameters passed to the planner kernels.
+struct PlanCfg {
+    long long target;         // particles kept in flight
+    int cap;                  // queue capacity
+    int lanes;                // resident threads of the transport kernels
+    int boost;                // largest budget multiplier as the queues drain (1 = fixed)
+    int tsteps;               // base electron budget (tstep-loop iterations)
 };
 
 struct EventState {
@@ -45,7 +56,10 @@ struct EventState {
     DBuf ctl;
     Ctl *ctl_d = nullptr;
     int block = 256;
-    int grid = 0;
+    int grid = 0;             // source kernels
+    int grid_p = 0, grid_e = 0;  // transport kernels: one wave of resident blocks
+    int lanes = 0;            // resident threads of the electron kernel
+    int boost = 32;           // budget multiplier limit in the drain tail
     int tsteps = 2;           // electron tstep iterations per event launch
     long long inflight = 0;   // particles kept in flight by the injector
     KernelProfile prof[4];    // 0 source, 1 photon, 2 electron, 3 plan+reset
@@ -86,6 +100,7 @@ int event_prepare(omc_engine *e);
 // One serving cycle with input buffers `in` (0 = A, 1 = B); tally slot of a
 // particle = request slot * nbmax + batch.
 void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
+PlanCfg plan_cfg(const omc_engine *e, long long target);
 
 int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint64_t seed, double *sum, double *sum2,
                    double *src_energy, KernelStats &ks);

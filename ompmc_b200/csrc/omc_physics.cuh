@@ -11,9 +11,10 @@
 //   R    float (event-based FP32 transport) or double (plain FP64 form)
 //   Env  the environment: R uni(); void deposit(int ir, R e);
 //        bool push(const Part<R>&); void err(unsigned); void cross() (a
-//        voxel boundary was crossed; counting only); int tstep_budget()
-//        (tstep-loop iterations one electron_step call may run before it
-//        returns the particle unchanged for a later call); bool tick() (false
+//        voxel boundary was crossed; counting only); bool tstep_take()
+//        (false once the caller's budget of tstep-loop iterations is spent:
+//        electron_step then returns the particle for a later call, which
+//        resumes it exactly); bool tick() (false
 //        once the history's transport-step budget is spent; every loop
 //        that could run away is bounded by it or by a local guard)
 //
@@ -35,10 +36,19 @@ struct Part {
 };
 
 // ------------------------------------------------------------ math shims
+// FP32 transport uses the hardware log2/exp2 based intrinsics (a few
+// instructions each instead of an inlined library routine at each of some
+// forty call sites); their errors (about 2^-21 absolute near 1) are far below
+// the FP32 transport's own rounding.
 OMC_HD double m_log(double x) { return log(x); }
-OMC_HD float m_log(float x) { return logf(x); }
 OMC_HD double m_exp(double x) { return exp(x); }
+#ifdef __CUDA_ARCH__
+OMC_HD float m_log(float x) { return __logf(x); }
+OMC_HD float m_exp(float x) { return __expf(x); }
+#else
+OMC_HD float m_log(float x) { return logf(x); }
 OMC_HD float m_exp(float x) { return expf(x); }
+#endif
 OMC_HD double m_sqrt(double x) { return sqrt(x); }
 OMC_HD float m_sqrt(float x) { return sqrtf(x); }
 OMC_HD double m_sin(double x) { return sin(x); }
@@ -51,6 +61,23 @@ template <typename R> OMC_HD R m_max(R a, R b) { return a > b ? a : (b == b ? b 
 template <typename R> OMC_HD R m_min(R a, R b) { return a < b ? a : (b == b ? b : a); }
 template <typename R> OMC_HD R sq(R x) { return x * x; }
 template <typename R> OMC_HD bool m_abs_lt(R a, R b) { return (a < R(0) ? -a : a) < b; }
+
+// FP32 transport renormalises a direction wherever it is rotated, so that
+// rounding drift never accumulates and the trajectory does not depend on
+// where events are cut; the FP64 form is left untouched (its trajectories
+// stay bit-identical to the reference's).
+OMC_HD void renorm_dir(double &, double &, double &) {}
+OMC_HD void renorm_dir(float &u, float &v, float &w) {
+    float n2 = u * u + v * v + w * w;
+    if (n2 > 0.f && fabsf(n2 - 1.f) > 1e-6f) {
+#ifdef __CUDA_ARCH__
+        float r = rsqrtf(n2);
+#else
+        float r = 1.0f / sqrtf(n2);
+#endif
+        u *= r; v *= r; w *= r;
+    }
+}
 
 template <typename R>
 OMC_HD R pwl(const PL<R> &p, R x) { return x * p.a1 + p.a0; }
@@ -193,6 +220,7 @@ OMC_HD void uphi21(Env &g, Part<R> &p, Uphi<R> &h, R costhe, R sinthe) {
     azimuth(g, h.cphi, h.sphi);
     h.A = p.u; h.B = p.v; h.C = p.w;
     rotate_into(h.A, h.B, h.C, costhe, sinthe, h.cphi, h.sphi, p.u, p.v, p.w);
+    renorm_dir(p.u, p.v, p.w);
 }
 
 // Partner particle: position, region and weight of p, direction rotated
@@ -201,6 +229,7 @@ template <typename R>
 OMC_HD Part<R> uphi32(const Part<R> &p, const Uphi<R> &h, R costhe, R sinthe) {
     Part<R> q = p;
     rotate_into(h.A, h.B, h.C, costhe, sinthe, h.cphi, h.sphi, q.u, q.v, q.w);
+    renorm_dir(q.u, q.v, q.w);
     return q;
 }
 
@@ -210,7 +239,7 @@ OMC_HD Part<R> uphi32(const Part<R> &p, const Uphi<R> &h, R costhe, R sinthe) {
 // `(int)rnno0*dwi` == 0 and the form-factor tables of medium 0 are used
 // for every medium.
 template <typename R, typename Env>
-OMC_HD void rayleigh(const DevData<R> &D, Env &g, Part<R> &p, int imed, R gle, int lgle) {
+OMC_COLD void rayleigh(const DevData<R> &D, Env &g, Part<R> &p, int imed, R gle, int lgle) {
     R eig = p.e;
     R pmax = pwl(D.pmax[imed * D_MXGE + (lgle < 0 ? 0 : (lgle > D_MXGE - 1 ? D_MXGE - 1 : lgle))], gle);
     R xmax = R(80.65506856998) * eig;
@@ -254,7 +283,7 @@ OMC_HD R pair_rej(R zbrang, R xi, R esedei, R eseder, R tteig) {
 // p becomes particle 1 and particle 2 is pushed.  quirk: the angle loop
 // accepts as soon as theta < pi.
 template <typename R, typename Env>
-OMC_HD void pair(const DevData<R> &D, Env &g, Part<R> &p, int imed) {
+OMC_COLD void pair(const DevData<R> &D, Env &g, Part<R> &p, int imed) {
     const MedS<R> &M = D.ms[imed];
     const R RMr = R(D_RM);
     R eig = p.e, ese1, ese2;
@@ -364,7 +393,7 @@ OMC_HD void pair(const DevData<R> &D, Env &g, Part<R> &p, int imed) {
 // Compton scattering off free electrons, Klein-Nishina (compton,
 // ompmc.c:1688-1801).  p stays the scattered photon; the electron is pushed.
 template <typename R, typename Env>
-OMC_HD void compton(const DevData<R> &D, Env &g, Part<R> &p) {
+OMC_COLD void compton(const DevData<R> &D, Env &g, Part<R> &p) {
     const R RMr = R(D_RM);
     R eig = p.e, ko = p.e / RMr;
     R broi = R(1) + R(2) * ko, bro = R(1) / broi;
@@ -432,7 +461,7 @@ OMC_HD void compton(const DevData<R> &D, Env &g, Part<R> &p) {
 // along the Sauter distribution when above the region's cut-off
 // (photo, ompmc.c:1804-1864).
 template <typename R, typename Env>
-OMC_HD void photo(const DevData<R> &D, Env &g, Part<R> &p) {
+OMC_COLD void photo(const DevData<R> &D, Env &g, Part<R> &p) {
     const R RMr = R(D_RM);
     p.e += RMr;
     p.iq = -1;
@@ -548,7 +577,7 @@ OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
 // Annihilation at rest: two back-to-back photons of m each; p becomes the
 // first and the second is pushed (rannih, ompmc.c:4129-4185).
 template <typename R, typename Env>
-OMC_HD void rannih(const DevData<R> &D, Env &g, Part<R> &p) {
+OMC_COLD void rannih(const DevData<R> &D, Env &g, Part<R> &p) {
     R rnno = g.uni();
     R costhe = R(2) * rnno - R(1);
     R sinthe = m_sqrt(m_max(R(0), (R(1) - costhe) * (R(1) + costhe)));
@@ -571,7 +600,7 @@ OMC_HD void rannih(const DevData<R> &D, Env &g, Part<R> &p) {
 // (Coulomb corrected above 50 MeV), photon angle from Koch-Motz 2BS
 // (brems, ompmc.c:4188-4374).  p keeps its direction; the photon is pushed.
 template <typename R, typename Env>
-OMC_HD void brems(const DevData<R> &D, Env &g, Part<R> &p) {
+OMC_COLD void brems(const DevData<R> &D, Env &g, Part<R> &p) {
     const R RMr = R(D_RM);
     int imed = D.med[p.ir];
     const MedS<R> &M = D.ms[imed];
@@ -665,7 +694,7 @@ OMC_HD void brems(const DevData<R> &D, Env &g, Part<R> &p) {
 // Moller scattering (moller, ompmc.c:4377-4453): p keeps energy ese1, the
 // delta ray (ese2) is pushed.
 template <typename R, typename Env>
-OMC_HD void moller(const DevData<R> &D, Env &g, Part<R> &p) {
+OMC_COLD void moller(const DevData<R> &D, Env &g, Part<R> &p) {
     const R RMr = R(D_RM);
     const MedS<R> &M = D.ms[D.med[p.ir]];
     R eie = p.e, ekin = eie - RMr;
@@ -701,7 +730,7 @@ OMC_HD void moller(const DevData<R> &D, Env &g, Part<R> &p) {
 // Bhabha scattering (bhabha, ompmc.c:4456-4543): the more energetic
 // particle stays the positron.
 template <typename R, typename Env>
-OMC_HD void bhabha(const DevData<R> &D, Env &g, Part<R> &p) {
+OMC_COLD void bhabha(const DevData<R> &D, Env &g, Part<R> &p) {
     const R RMr = R(D_RM);
     const MedS<R> &M = D.ms[D.med[p.ir]];
     R eip = p.e, ekin = eip - RMr;
@@ -747,7 +776,7 @@ OMC_HD void bhabha(const DevData<R> &D, Env &g, Part<R> &p) {
 
 // Two-photon annihilation in flight, Heitler (annih, ompmc.c:4546-4663).
 template <typename R, typename Env>
-OMC_HD void annih(const DevData<R> &D, Env &g, Part<R> &p) {
+OMC_COLD void annih(const DevData<R> &D, Env &g, Part<R> &p) {
     const R RMr = R(D_RM);
     R avip = p.e + RMr;
     R a = avip / RMr;
@@ -809,7 +838,7 @@ struct SpinIdx {
 // (spinRejection, ompmc.c:3115-3185).  Indices are clamped to the table
 // (the reference reads one element past a row at the edges).
 template <typename R, typename Env>
-OMC_HD R spin_rej(const DevData<R> &D, Env &g, int imed, int qel, R elke, R beta2, R q1, R cost,
+OMC_OUTLINE R spin_rej(const DevData<R> &D, Env &g, int imed, int qel, R elke, R beta2, R q1, R cost,
                   bool &spin_index, bool is_single, SpinIdx &si) {
     if (spin_index) {
         spin_index = false;
@@ -867,7 +896,7 @@ struct MsIdx {
 // surface's in-bin slope du is ums[k]-ums[k] (zero), so u is one of the 32
 // nodes; ref_compat = 0 uses ums[k+1]-ums[k].
 template <typename R, typename Env>
-OMC_HD void mscat(const DevData<R> &D, Env &g, int imed, int qel, bool &spin_index, bool &find_index, R elke,
+OMC_OUTLINE void mscat(const DevData<R> &D, Env &g, int imed, int qel, bool &spin_index, bool &find_index, R elke,
                   R beta2, R q1, R lambda, R chia2, R &cost, R &sint, MsIdx &mi, R &omega2, SpinIdx &si) {
     R explambda = m_exp(-lambda);
     if (lambda <= R(13.8)) {
@@ -993,7 +1022,7 @@ OMC_HD void mscat(const DevData<R> &D, Env &g, int imed, int qel, bool &spin_ind
 
 // Single elastic scattering with spin rejection (sscat, ompmc.c:3188-3217).
 template <typename R, typename Env>
-OMC_HD void sscat(const DevData<R> &D, Env &g, int imed, int qel, R chia2, R elke, R beta2, R &cost, R &sint) {
+OMC_COLD void sscat(const DevData<R> &D, Env &g, int imed, int qel, R chia2, R elke, R beta2, R &cost, R &sint) {
     bool spin_index = true;
     SpinIdx si{0, 0};
     R xi, rejf, rnno;
@@ -1111,7 +1140,7 @@ OMC_HD R msdist(const DevData<R> &D, Env &g, const Part<R> &p, int imed, int iq,
 // Path length from ekei down to ekef inside one interval of the log-linear
 // stopping-power table (computeDrange, ompmc.c:3997-4033).
 template <typename R>
-OMC_HD R drange(const DevData<R> &D, int imed, int qel, int lelke, R ekei, R ekef, R elkei, R elkef) {
+OMC_OUTLINE R drange(const DevData<R> &D, int imed, int qel, int lelke, R ekei, R ekef, R elkei, R elkef) {
     R fedep = R(1) - ekef / ekei;
     R elktmp = R(0.5) * (elkei + elkef + R(0.25) * fedep * fedep * (R(1) + fedep * (R(1) + R(0.875) * fedep)));
     const ElBin<R> &B = ebin(D, imed, qel, lelke);
@@ -1125,7 +1154,7 @@ OMC_HD R drange(const DevData<R> &D, int imed, int qel, int lelke, R ekei, R eke
 // Energy lost to sub-threshold processes over path tustep (computeEloss,
 // ompmc.c:4036-4126).
 template <typename R>
-OMC_HD R eloss(const DevData<R> &D, int imed, int qel, R rhof, R tustep, R range, R eke, R elke, int lelke) {
+OMC_OUTLINE R eloss(const DevData<R> &D, int imed, int qel, R rhof, R tustep, R range, R eke, R elke, int lelke) {
     const MedS<R> &M = D.ms[imed];
     R tuss = range - ebin(D, imed, qel, lelke).range / rhof;
     R de;
@@ -1167,7 +1196,7 @@ enum EStep : int { E_DEAD = 0, E_ALIVE = 1 };
 // Electron/positron below its cut-off: deposit the kinetic energy; a
 // positron annihilates at rest (ompmc.c:4683-4705 and repeats).
 template <typename R, typename Env>
-OMC_HD int e_cutoff(const DevData<R> &D, Env &g, Part<R> &p, R eie) {
+OMC_COLD int e_cutoff(const DevData<R> &D, Env &g, Part<R> &p, R eie) {
     R edep = p.e - R(D_RM);
     g.deposit(p.ir, p.wt * edep);
     if (p.iq > 0 && edep < eie) {
@@ -1199,13 +1228,11 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
     R sig0 = 0, demfp = 0, total_de = 0, total_tstep = 0;
     R ustep = 0;
     int guard = 0;
-    int ntstep = 0;
-    const int tstep_budget = g.tstep_budget();
     for (;;) {  // tstep loop
         // The top of the tstep loop carries no state but the particle
         // (demfp is re-drawn here), so an event can stop after a budget of
         // iterations and resume in a later launch exactly where it was.
-        if (ntstep++ >= tstep_budget) return E_ALIVE;
+        if (!g.tstep_take()) return E_ALIVE;
         bool compute_tstep = true;
         R eke = eie - RMr;
         if (imed != -1) {
@@ -1397,6 +1424,7 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
             g.deposit(p.ir, p.wt * edep);
             p.x = xf; p.y = yf; p.z = zf;
             p.u = uf; p.v = vf; p.w = wf;
+            renorm_dir(p.u, p.v, p.w);
             irold = p.ir;
             eie -= edep;
             p.e = eie;

@@ -43,7 +43,7 @@ struct PlainEnv {
     }
     __device__ void err(unsigned f) { flags |= f; }
     __device__ void cross() {}
-    __device__ int tstep_budget() const { return 1 << 30; }
+    __device__ bool tstep_take() const { return true; }
 };
 
 // shower() (ompmc.c:5454-5465) on a local stack.
@@ -188,7 +188,7 @@ struct ReplayEnv {
     }
     __device__ void err(unsigned f) { flags |= f; }
     __device__ void cross() {}
-    __device__ int tstep_budget() const { return 1 << 30; }
+    __device__ bool tstep_take() const { return true; }
 };
 
 __global__ void k_replay(DevData<double> D, const double *prim, int nhist, const double *rn, const long *rn_off,

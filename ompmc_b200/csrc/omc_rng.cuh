@@ -55,19 +55,33 @@ struct Philox {
     uint32_t k0, k1, ctr, seedw;
     U4 buf;
     int pos;
-    OMC_HD void init(uint64_t key, uint32_t seed_word, uint32_t counter = 0) {
+    // Stream `key` positioned after `position` numbers were drawn from it:
+    // a particle that stops mid-block resumes with the next number of that
+    // block, so its stream does not depend on where events are cut.
+    OMC_HD void init(uint64_t key, uint32_t seed_word, uint32_t position = 0) {
         k0 = (uint32_t)key;
         k1 = (uint32_t)(key >> 32);
         seedw = seed_word;
-        ctr = counter;
-        pos = 4;
-    }
-    OMC_HD uint32_t next32() {
-        if (pos >= 4) {
+        ctr = position >> 2;
+        pos = (int)(position & 3u);
+        if (pos == 0) {
+            pos = 4;
+        } else {
             buf = philox4x32_10(U4{ctr, seedw, 0x6f6d6321u, 0u}, k0, k1);
             ctr++;
-            pos = 0;
         }
+    }
+    // Numbers drawn so far (the argument init() resumes from).
+    OMC_HD uint32_t position() const { return (ctr << 2) - 4u + (uint32_t)pos; }
+    // The block generator runs once per four numbers; one out-of-line copy
+    // instead of one per draw site keeps the transport kernels small.
+    __host__ __device__ __noinline__ void refill() {
+        buf = philox4x32_10(U4{ctr, seedw, 0x6f6d6321u, 0u}, k0, k1);
+        ctr++;
+        pos = 0;
+    }
+    OMC_HD uint32_t next32() {
+        if (pos >= 4) refill();
         uint32_t v = pos == 0 ? buf.x : pos == 1 ? buf.y : pos == 2 ? buf.z : buf.w;
         pos++;
         return v;

@@ -570,7 +570,7 @@ int omc_run_beamlets(omc_engine *e, const omc_beamlets *b, int64_t nhist, int nb
             cvar[i] = std::move(r.var);
             histories += r.nhist;
         }
-        launches = (double)s->cycles * 5;
+        launches = (double)s->cycles * 4;
     } else if (mode == OMC_PLAIN_FP64) {
         PlanBuf pb;
         if ((rc = upload_plan<double>(e, b, pb.f64, pb.s64))) return rc;

@@ -50,7 +50,7 @@ class _Options(C.Structure):
     _fields_ = [("ecut", C.c_double), ("pcut", C.c_double), ("device", C.c_int),
                 ("ref_compat", C.c_int), ("queue_capacity", C.c_int64), ("block", C.c_int),
                 ("nsplit", C.c_int), ("profile", C.c_int), ("electron_tsteps", C.c_int),
-                ("inflight", C.c_int64)]
+                ("inflight", C.c_int64), ("tail_boost", C.c_int)]
 
 
 class _Energy(C.Structure):
@@ -194,7 +194,7 @@ class Engine:
     """Resident tables + phantom on one GPU."""
 
     def __init__(self, tables: Tables, phantom, ecut=0.7, pcut=0.01, device=0, ref_compat=True,
-                 queue_capacity=0, block=0, profile=False, electron_tsteps=0, inflight=0):
+                 queue_capacity=0, block=0, profile=False, electron_tsteps=0, inflight=0, tail_boost=0):
         L = lib()
         self.tables = tables
         self.phantom = phantom
@@ -216,6 +216,7 @@ class Engine:
         o.profile = 1 if profile else 0
         o.electron_tsteps = electron_tsteps
         o.inflight = inflight
+        o.tail_boost = tail_boost
         h = C.c_void_p()
         _check(L.omc_engine_create(tables.h, C.byref(P), C.byref(o), C.byref(h)))
         self.h = h
@@ -331,7 +332,7 @@ class Engine:
         """Per-kernel profile of the last profiled event-form run."""
         out = np.zeros(28)
         _check(lib().omc_profile_last(self.h, _p(out, _dp), 28), self.h)
-        names = ["source", "photon", "electron", "plan_reset"]
+        names = ["source", "photon", "electron", "plan"]
         keys = ["launches", "seconds", "particles", "steps", "cross", "dep", "atom"]
         return {names[k]: dict(zip(keys, out[k * 7:(k + 1) * 7])) for k in range(4)}
 
