@@ -244,6 +244,21 @@ def bench_serving(device, nbeamlets, load=0.7, seed=7, plain_sample=12):
             "speedup_served_vs_plain": served / plain}
 
 
+def reduce_max(vals, dist, device):
+    """Element-wise maximum over ranks (the job's time is its slowest rank)."""
+    if dist is None:
+        return [float(v) for v in vals]
+    import torch
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def rank_seed(rank):
+    """Base seed of a rank's histories: every rank (replica) gets its own."""
+    return 1000003 * (rank + 1)
+
+
 def host_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -297,6 +312,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and plain comparator")
     ap.add_argument("--serving-requests", type=int, default=300,
                     help="beamlet requests in the serving workload (0 skips it)")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch parameters)")
     ap.add_argument("--cycle-trace", action="store_true",
                     help="print the per-cycle trace (queue sizes, kernel ms) of the first warm-up step and exit")
     args = ap.parse_args()
@@ -320,7 +336,7 @@ def main():
     eng = Engine(tables, ph, ecut=0.7, pcut=0.01, device=local)
     mode = EVENT_FP32 if args.mode == "event" else PLAIN_FP64
     nstep = args.hist_per_step
-    seed0 = 1000003 * (rank + 1)
+    seed0 = rank_seed(rank)
 
     def step(i, e=eng, m=mode, n=nstep):
         return e.run_beam(n, NBATCH, seed=seed0 + i, mode=m, spectrum=spec, collimator=COLLIMATOR)
@@ -336,6 +352,13 @@ def main():
         print(json.dumps({"seed": seed0 - 1, "histories": nstep, "columns": cols, "cycles": rows.tolist()}))
         eng.close()
         return 0
+    tuned = None
+    if not args.no_tune:
+        # launch parameters picked by the autotuner on 10^6-history runs of
+        # the same beam (untimed; results do not depend on them)
+        from ompmc_b200.autotune import tune_beam
+        cfg, rate, trials = tune_beam(eng, nhist=min(nstep, 1_000_000), spectrum=spec, collimator=COLLIMATOR)
+        tuned = dict(cfg, trials=len(trials), tune_hist_per_s=rate)
     for i in range(args.warmup):
         step(-1 - i)
     sampler = ClockSampler(local)
@@ -357,10 +380,7 @@ def main():
     if dist:
         dist.barrier()
     clocks = sampler.stop()
-    if dist:
-        t = torch.tensor([dev_s, wall], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_s, wall = float(t[0]), float(t[1])
+    dev_s, wall = reduce_max([dev_s, wall], dist, "cuda")
     total = nstep * args.steps * world
     value = total / dev_s
     e2e = total / wall
@@ -371,6 +391,8 @@ def main():
         # roofline of the dominant kernel from a profiled (untimed) step
         peak, peak_kind = peaks()
         prof_eng = Engine(tables, ph, ecut=0.7, pcut=0.01, device=local, profile=True)
+        if tuned:
+            prof_eng.event_params(**{k: tuned[k] for k in ("electron_tsteps", "tail_boost", "inflight", "block")})
         prof_eng.run_beam(nstep, NBATCH, seed=777, mode=EVENT_FP32, spectrum=spec, collimator=COLLIMATOR)
         prof = prof_eng.profile_last()
         prof_eng.close()
@@ -434,7 +456,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if mode == EVENT_FP32 else "f64",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "mode": args.mode, "histories_per_step_per_gpu": nstep,
-                       "tally": "f64", "parallelism": f"replicas{world}",
+                       "tally": "f64", "parallelism": f"replicas{world}", "tuned": tuned,
                        "l2": "particle queues (0.8 GB) and batch tallies exceed L2; physics tables are L2-resident"},
             "e2e": {"value": e2e, "unit": "histories/s", "h2d_bytes_per_step": 2 * 1000 * 8 + 64,
                     "d2h_bytes_per_step": 2 * nvox * 8},

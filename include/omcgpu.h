@@ -77,7 +77,8 @@ typedef struct {
     int device;           /* CUDA device ordinal */
     int ref_compat;       /* 1: reproduce ompMC's sampling quirks (default) */
     int64_t queue_capacity; /* event form: particles per queue (0 = default) */
-    int block;            /* threads per block (0 = default) */
+    int block;            /* threads per block (0 = default; event form: a
+                             multiple of 32, at most 256) */
     int nsplit;           /* photon splitting: only 1 is supported */
     int profile;          /* 1: event form launches cycles one by one and times
                              every kernel (see omc_profile_last) */
@@ -95,6 +96,11 @@ typedef struct omc_engine omc_engine;
 /* Uploads tables and phantom once; they stay resident across runs. */
 int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_options *o, omc_engine **out);
 int omc_engine_destroy(omc_engine *e);
+/* Event-form tuning parameters of a live engine (the options of the same
+ * names; a value <= 0 keeps the current one).  Results do not depend on
+ * them (up to the summation order of the FP64 tallies); the autotuner
+ * (ompmc_b200/autotune.py) sweeps them. */
+int omc_event_params(omc_engine *e, int electron_tsteps, int tail_boost, int64_t inflight, int block);
 const char *omc_engine_last_error(const omc_engine *e);
 
 /* Per-kernel profile of the last event-form omc_run_beam made with

@@ -544,6 +544,12 @@ int omc_engine_destroy(omc_engine *e) {
 
 const char *omc_engine_last_error(const omc_engine *e) { return e ? e->err.c_str() : omc_last_error(); }
 
+int omc_event_params(omc_engine *e, int electron_tsteps, int tail_boost, int64_t inflight, int block) {
+    if (!e) return global_err(OMC_E_ARG, "omc_event_params: null engine");
+    cudaSetDevice(e->device);
+    return event_set_params(e, electron_tsteps, tail_boost, (long long)inflight, block);
+}
+
 int omc_profile_last(const omc_engine *e, double *out, int n) {
     if (!e || !out || n < 28) return global_err(OMC_E_ARG, "omc_profile_last: bad argument");
     for (int i = 0; i < 28; i++) out[i] = 0;

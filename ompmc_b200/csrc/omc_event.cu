@@ -31,6 +31,7 @@ namespace omc {
 
 constexpr int EV_BUDGET = 200000;  // transport steps one event may take
 constexpr int EV_MAXOUT = 1;       // secondaries an event emits: every interaction sampler pushes one
+constexpr int EV_MAX_BLOCK = 256;  // launch bound of the transport kernels
 
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
@@ -250,7 +251,7 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
 
 // Photon events of the queued photons.  `live` (may be null) receives the
 // change of each serving request's live-particle count.
-__global__ void __launch_bounds__(256) k_photon_step(DevData<float> D, Queue in, Queue outP, Queue outE,
+__global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_step(DevData<float> D, Queue in, Queue outP, Queue outE,
                                                      double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
                                                      int *live, int nbmax) {
     transport_events<true>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax);
@@ -259,7 +260,7 @@ __global__ void __launch_bounds__(256) k_photon_step(DevData<float> D, Queue in,
 // Electron/positron events of the queued charged particles: at most the
 // cycle's budget of tstep-loop iterations each, then the particle is
 // re-queued.
-__global__ void __launch_bounds__(256) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
+__global__ void __launch_bounds__(EV_MAX_BLOCK) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
                                                        double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
                                                        int *live, int nbmax) {
     transport_events<false>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax);
@@ -351,8 +352,9 @@ int event_prepare(omc_engine *e) {
     EventState &S = *e->ev;
     long cap = e->opt.queue_capacity > 0 ? e->opt.queue_capacity : (1L << 22);
     S.cap = (int)std::min(cap, (long)(1L << 30));
-    // warps fetch work 32 particles at a time: whole warps per block
-    S.block = e->opt.block > 0 ? std::min(1024, (e->opt.block + 31) / 32 * 32) : 256;
+    // warps fetch work 32 particles at a time: whole warps per block, at
+    // most the transport kernels' launch bound
+    S.block = e->opt.block > 0 ? std::min(EV_MAX_BLOCK, (e->opt.block + 31) / 32 * 32) : 256;
     S.grid = e->sm_count * std::max(1, 2048 / S.block);
     int bp = 0, be = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_photon_step, S.block, 0);
@@ -370,6 +372,34 @@ int event_prepare(omc_engine *e) {
     for (int i = 0; i < 4; i++)
         if ((rc = alloc_queue(e, S.buf[i], S.q[i], S.cap, &S.ctl_d->cnt[i]))) return rc;
     S.ready = true;
+    return OMC_OK;
+}
+
+// Event-form tuning parameters of an engine (values <= 0 keep the current
+// one); the queues are not reallocated.
+int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, int block) {
+    if (tsteps > 0) e->opt.electron_tsteps = tsteps;
+    if (boost > 0) e->opt.tail_boost = boost;
+    if (inflight > 0) e->opt.inflight = inflight;
+    if (block > 0) {
+        if (block % 32 || block > EV_MAX_BLOCK)
+            return set_err(e, OMC_E_ARG, "block must be a multiple of 32, at most 256");
+        e->opt.block = block;
+    }
+    if (e->ev && e->ev->ready) {
+        EventState &S = *e->ev;
+        S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 2;
+        S.boost = e->opt.tail_boost > 0 ? e->opt.tail_boost : 32;
+        S.inflight = e->opt.inflight > 0 ? e->opt.inflight : (1LL << 20);
+        S.block = e->opt.block > 0 ? std::min(EV_MAX_BLOCK, e->opt.block) : 256;
+        S.grid = e->sm_count * std::max(1, 2048 / S.block);
+        int bp = 0, be = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_photon_step, S.block, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, k_electron_step, S.block, 0);
+        S.grid_p = e->sm_count * std::max(1, bp);
+        S.grid_e = e->sm_count * std::max(1, be);
+        S.lanes = S.grid_e * S.block;
+    }
     return OMC_OK;
 }
 

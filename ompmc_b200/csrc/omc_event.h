@@ -101,6 +101,7 @@ int event_prepare(omc_engine *e);
 // particle = request slot * nbmax + batch.
 void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
 PlanCfg plan_cfg(const omc_engine *e, long long target);
+int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, int block);
 
 int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint64_t seed, double *sum, double *sum2,
                    double *src_energy, KernelStats &ks);

@@ -101,6 +101,7 @@ def lib():
         "omc_dosxyz_run": ([C.c_char_p, C.c_char_p, C.c_int, C.c_int], C.c_int),
         "omc_profile_last": ([C.c_void_p, _dp, C.c_int], C.c_int),
         "omc_profile_trace": ([C.c_void_p, _dp, C.c_int], C.c_int),
+        "omc_event_params": ([C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int], C.c_int),
         "omc_run_beam_noalloc": ([C.c_void_p, C.POINTER(_Beam), C.c_int64, C.c_int, C.c_uint64, _dp, _dp, _dp],
                                  C.c_int),
         "omc_server_create": ([C.c_void_p, C.c_int64, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)], C.c_int),
@@ -337,6 +338,11 @@ class Engine:
         return {names[k]: dict(zip(keys, out[k * 7:(k + 1) * 7])) for k in range(4)}
 
     # ------------------------------------------------ validation hooks
+    def event_params(self, electron_tsteps=0, tail_boost=0, inflight=0, block=0):
+        """Event-form tuning parameters (0 keeps the current value)."""
+        _check(lib().omc_event_params(self.h, int(electron_tsteps), int(tail_boost), int(inflight), int(block)),
+               self.h)
+
     def profile_trace(self):
         """Per-cycle trace of the last profiled event-form run: array of rows
         (injected, photons in, electrons in, source ms, photon ms, electron ms)."""

@@ -10,8 +10,13 @@ Fixtures (all seeded; reference RNG seeds 97 33, one thread):
   replay_<case>.npz   primaries, the uniform stream each history consumed
                       (stored exactly as integers rn * 2^24, RANMAR's
                       resolution) and its deposit sequence (region, energy)
-  dose_<case>.npz     reference CLI dose and relative uncertainty of the
-                      voxels above 5 % of the maximum (8 threads, 2e6 histories in 50 batches)
+  dose*_<case>.npz    reference CLI dose and relative uncertainty of the
+                      voxels above 5 % of the maximum (8 threads, 50 batches;
+                      sources in DOSE: 6 MV and 18 MV photon spectra, 6 MeV
+                      electrons, 3 MeV positrons)
+  gamma_<case>.npz    high-statistics reference CLI dose of the voxels above
+                      2 % of the maximum for the gamma 2 %/2 mm test (8 threads;
+                      water30 1e8, slab64 4e8 histories in 100 batches)
   (the table comparison runs against the live oracle; no fixture)
 Cases: water30 (30^3 x 1 cm water), slab64 (64^3 x 0.25 cm water/lung/bone),
 ctsmall (32x32x24 x 1.2 cm CT-like, 4 media).
@@ -130,13 +135,52 @@ def _tables(name, out):
     np.savez_compressed(out, **d)
 
 
-def make_dose(name, ncase=2000000, nbatch=50, cores=8):
+# Dose fixtures: name -> (case, spectrum or None, mono energy MeV, charge, histories)
+DOSE = {
+    "dose_water30": ("water30", "6mv", 1.25, 0, 2_000_000),
+    "dose_slab64": ("slab64", "6mv", 1.25, 0, 2_000_000),
+    "dose18_slab64": ("slab64", "18mv", 1.25, 0, 2_000_000),
+    "dose_ctsmall": ("ctsmall", "6mv", 1.25, 0, 2_000_000),
+    "dosee_water30": ("water30", None, 6.0, -1, 1_000_000),
+    "dosep_water30": ("water30", None, 3.0, 1, 1_000_000),
+}
+
+
+def make_dose(fixture, nbatch=50, cores=8):
+    """Reference CLI dose of one DOSE entry (voxels above 5 % of the max)."""
     from oracle.ref import run_cli
-    base, ph = case_inp(name, ncase=ncase, nbatch=nbatch)
-    loop_s, _ = run_cli(base, f"golden_{name}", cores=cores)
-    dose, unc, _ = A.read_3ddose(A.ASSETS / "out" / f"golden_{name}.3ddose")
+    name, spectrum, mono, charge, ncase = DOSE[fixture]
+    A.require_assets()
+    c = CASES[name]
+    ph = c["phantom"]()
+    pf = WORK / f"{name}.egsphant"
+    if not pf.exists():
+        A.write_egsphant(pf, ph)
+    run = A.default_run(pf, spectrum=spectrum, ncase=ncase, nbatch=nbatch, collimator=c["collimator"],
+                        mono_energy=mono, charge=charge)
+    base = WORK / f"{fixture}_{ncase}"
+    A.write_inp(base, run)
+    loop_s, _ = run_cli(base, f"golden_{fixture}", cores=cores)
+    dose, unc, _ = A.read_3ddose(A.ASSETS / "out" / f"golden_{fixture}.3ddose")
     keep = np.flatnonzero(dose.ravel() > 0.05 * dose.max())
-    np.savez_compressed(HERE / f"dose_{name}.npz", idx=keep.astype(np.int32), dose=dose.ravel()[keep],
+    np.savez_compressed(HERE / f"{fixture}.npz", idx=keep.astype(np.int32), dose=dose.ravel()[keep],
+                        unc=unc.ravel()[keep].astype(np.float32), shape=np.array(dose.shape), dmax=dose.max(),
+                        ncase=ncase, nbatch=nbatch, loop_seconds=loop_s, cores=cores,
+                        spectrum=str(spectrum or ""), mono_energy=mono, charge=charge)
+
+
+GAMMA_HIST = {"water30": 100_000_000, "slab64": 400_000_000}
+
+
+def make_gamma(name, nbatch=100, cores=8):
+    """High-statistics reference dose for the gamma comparison."""
+    from oracle.ref import run_cli
+    ncase = GAMMA_HIST[name]
+    base, ph = case_inp(name, ncase=ncase, nbatch=nbatch)
+    loop_s, _ = run_cli(base, f"gamma_{name}", cores=cores, timeout=6 * 3600)
+    dose, unc, _ = A.read_3ddose(A.ASSETS / "out" / f"gamma_{name}.3ddose")
+    keep = np.flatnonzero(dose.ravel() > 0.02 * dose.max())
+    np.savez_compressed(HERE / f"gamma_{name}.npz", idx=keep.astype(np.int32), dose=dose.ravel()[keep],
                         unc=unc.ravel()[keep].astype(np.float32), shape=np.array(dose.shape), dmax=dose.max(),
                         ncase=ncase, nbatch=nbatch, loop_seconds=loop_s, cores=cores)
 
@@ -184,11 +228,16 @@ def main():
             continue
         print("generating", fn, flush=True)
         _in_subprocess(name, what, HERE / f"{fn}.npz")
-    for name in ("water30", "slab64"):
-        if a.only and a.only not in f"dose_{name}":
+    for fixture in DOSE:
+        if a.only and a.only not in fixture:
             continue
-        print("generating dose", name, flush=True)
-        make_dose(name)
+        print("generating", fixture, flush=True)
+        make_dose(fixture)
+    for name in GAMMA_HIST:
+        if a.only and a.only not in f"gamma_{name}":
+            continue
+        print("generating gamma reference", name, flush=True)
+        make_gamma(name)
     if not a.only or a.only in "dij_ctsmall":
         print("generating dij_ctsmall", flush=True)
         make_dij()
