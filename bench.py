@@ -392,7 +392,8 @@ def main():
         peak, peak_kind = peaks()
         prof_eng = Engine(tables, ph, ecut=0.7, pcut=0.01, device=local, profile=True)
         if tuned:
-            prof_eng.event_params(**{k: tuned[k] for k in ("electron_tsteps", "tail_boost", "inflight", "block")})
+            prof_eng.event_params(**{k: tuned[k] for k in ("electron_tsteps", "tail_boost", "inflight", "block",
+                                                           "electron_split")})
         prof_eng.run_beam(nstep, NBATCH, seed=777, mode=EVENT_FP32, spectrum=spec, collimator=COLLIMATOR)
         prof = prof_eng.profile_last()
         prof_eng.close()

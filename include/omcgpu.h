@@ -70,6 +70,7 @@ typedef struct {
 /* ------------------------------------------------------------ engine */
 #define OMC_PLAIN_FP64 0   /* history-based, one thread per history, FP64 */
 #define OMC_EVENT_FP32 1   /* event-based queues, FP32 transport, FP64 tallies */
+#define OMC_MAX_NSPLIT 64  /* largest photon splitting factor (omc_options.nsplit) */
 
 typedef struct {
     double ecut;          /* global ecut, total energy (MeV) ("global ecut") */
@@ -79,7 +80,10 @@ typedef struct {
     int64_t queue_capacity; /* event form: particles per queue (0 = default) */
     int block;            /* threads per block (0 = default; event form: a
                              multiple of 32, at most 256) */
-    int nsplit;           /* photon splitting: only 1 is supported */
+    int nsplit;           /* photon splitting factor, 1 (off) to OMC_MAX_NSPLIT;
+                             each photon interaction is sampled nsplit times at
+                             weight 1/nsplit, photons from electrons are played
+                             Russian roulette (ompmc.c:1867-2139, 4169-4182) */
     int profile;          /* 1: event form launches cycles one by one and times
                              every kernel (see omc_profile_last) */
     int electron_tsteps;  /* event form: tstep-loop iterations an electron runs
@@ -88,6 +92,10 @@ typedef struct {
     int tail_boost;       /* event form: largest factor by which event budgets
                              grow as the queues drain (0 = default 32, 1 = fixed
                              budgets); results do not depend on it */
+    double electron_split; /* event form: electrons above this kinetic energy
+                             (MeV) are queued apart from the others so that
+                             warps see particles of one kind (0 = one group,
+                             default 0.3); results do not depend on it */
 } omc_options;
 
 void omc_options_default(omc_options *o);
@@ -97,10 +105,11 @@ typedef struct omc_engine omc_engine;
 int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_options *o, omc_engine **out);
 int omc_engine_destroy(omc_engine *e);
 /* Event-form tuning parameters of a live engine (the options of the same
- * names; a value <= 0 keeps the current one).  Results do not depend on
+ * names; a value <= 0 keeps the current one, for electron_split < 0).  Results do not depend on
  * them (up to the summation order of the FP64 tallies); the autotuner
  * (ompmc_b200/autotune.py) sweeps them. */
-int omc_event_params(omc_engine *e, int electron_tsteps, int tail_boost, int64_t inflight, int block);
+int omc_event_params(omc_engine *e, int electron_tsteps, int tail_boost, int64_t inflight, int block,
+                     double electron_split);
 const char *omc_engine_last_error(const omc_engine *e);
 
 /* Per-kernel profile of the last event-form omc_run_beam made with
@@ -188,7 +197,10 @@ int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, ui
  * Every call shares the array and clears it at its start: calls that
  * overlap on the GPU (other threads, other engines on the same device)
  * race.  Arguments and results are those of omc_run_beam with mode
- * OMC_PLAIN_FP64; stats[1] is host wall time of the run. */
+ * OMC_PLAIN_FP64; stats[1] is host wall time of the run.  Engines with
+ * photon splitting (nsplit > 1) are rejected with OMC_E_RANGE: their
+ * kernels need a deeper per-thread stack, which the driver may grow on
+ * first launch. */
 #define OMC_NOALLOC_MAX_VOXELS 262144
 int omc_run_beam_noalloc(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, uint64_t seed, double *dose,
                          double *unc, double *stats);

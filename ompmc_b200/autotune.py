@@ -10,7 +10,9 @@ for speed per phantom, source and GPU:
 * tail_boost      — how far that budget may grow as the queues drain;
 * inflight        — particles kept in the queues by the injector;
 * block           — threads per block of the transport kernels (whole warps,
-                    at most 256, their launch bound).
+                    at most 256, their launch bound);
+* electron_split  — regroup energy: electrons above it (kinetic, MeV) are
+                    queued apart from the others (0 = one group).
 
 `tune_beam` runs short dose runs of the given beam on a live engine and
 searches the space coordinate by coordinate (each parameter swept with the
@@ -29,8 +31,9 @@ SPACE = {
     "tail_boost": [1, 8, 32, 128],
     "inflight": [1 << 18, 1 << 19, 1 << 20, 1 << 21],
     "block": [64, 128, 256],
+    "electron_split": [0.0, 0.2, 0.3, 0.5, 1.0],
 }
-DEFAULT = {"electron_tsteps": 2, "tail_boost": 32, "inflight": 1 << 20, "block": 256}
+DEFAULT = {"electron_tsteps": 2, "tail_boost": 32, "inflight": 1 << 20, "block": 256, "electron_split": 0.3}
 
 
 def _rate(eng, cfg, nhist, run_kw, repeats):

@@ -93,6 +93,7 @@ struct DevData {
     const R *spin;                   // [nmed][2][32][16][32]
     R b2spin_min, dbeta2i, espml, dleneri, dqq1i, dllambi, dqmsi;
     int ref_compat;                  // reproduce reference quirks (default 1)
+    int nsplit;                      // photon splitting factor (1 = off)
 };
 
 // Beam source of the dosxyz ucode (omc_dosxyz.c:337-632, :964-1068).

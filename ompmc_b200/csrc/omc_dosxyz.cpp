@@ -74,10 +74,7 @@ extern "C" int omc_dosxyz_run(const char *inp_base, const char *out_name, int mo
     opt.pcut = std::atof(v.c_str());
     if (!need(in, "nsplit", v)) return fail(OMC_E_ARG, "Can not find 'nsplit' key on input file.");
     opt.nsplit = std::atoi(v.c_str());
-    if (opt.nsplit > 1) {
-        omc_tables_free(tab);
-        return fail(OMC_E_RANGE, "photon splitting (nsplit > 1) is not supported by this engine");
-    }
+    if (opt.nsplit > 1 && verbose) std::printf("Photon splitting enabled, nsplit = %d\n", opt.nsplit);
 
     // source (initSource, omc_dosxyz.c:337-632)
     omc_beam beam{};

@@ -76,6 +76,7 @@ void make_layout(const Tables &t, const Phantom &ph, const Regions &rg, double e
     d.ny = ph.ny;
     d.nz = ph.nz;
     d.ref_compat = ref_compat;
+    d.nsplit = 1;
     L.xb.assign(ph.xb.begin(), ph.xb.end());
     L.yb.assign(ph.yb.begin(), ph.yb.end());
     L.zb.assign(ph.zb.begin(), ph.zb.end());
@@ -193,6 +194,7 @@ static int build_devset(omc_engine *e, DevSet<R> &S) {
     if ((rc = upload(e, S.spin, L.spin))) return rc;
     S.d = L.d;
     DevData<R> &d = S.d;
+    d.nsplit = e->opt.nsplit > 1 ? e->opt.nsplit : 1;
     d.xb = S.xb.template as<R>(); d.yb = S.yb.template as<R>(); d.zb = S.zb.template as<R>();
     d.med = S.med.template as<int8_t>(); d.rhof = S.rhof.template as<R>();
     d.ms = S.ms.template as<MedS<R>>(); d.ph = S.ph.template as<PhBin<R>>(); d.pmax = S.pmax.template as<PL<R>>();
@@ -473,6 +475,7 @@ void omc_options_default(omc_options *o) {
     o->queue_capacity = 0;
     o->block = 0;
     o->nsplit = 1;
+    o->electron_split = 0.3;
 }
 
 int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_options *o, omc_engine **out) {
@@ -483,7 +486,9 @@ int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_opti
     omc_options opt;
     omc_options_default(&opt);
     if (o) opt = *o;
-    if (opt.nsplit > 1) return global_err(OMC_E_RANGE, "photon splitting (nsplit > 1) is not supported");
+    if (opt.nsplit < 1) return global_err(OMC_E_ARG, "nsplit must be >= 1");
+    if (opt.nsplit > OMC_MAX_NSPLIT)
+        return global_err(OMC_E_RANGE, "nsplit above " + std::to_string(OMC_MAX_NSPLIT) + " is not supported");
     int ndev = 0;
     cudaError_t cr = cudaGetDeviceCount(&ndev);
     if (cr != cudaSuccess || ndev == 0)
@@ -544,10 +549,11 @@ int omc_engine_destroy(omc_engine *e) {
 
 const char *omc_engine_last_error(const omc_engine *e) { return e ? e->err.c_str() : omc_last_error(); }
 
-int omc_event_params(omc_engine *e, int electron_tsteps, int tail_boost, int64_t inflight, int block) {
+int omc_event_params(omc_engine *e, int electron_tsteps, int tail_boost, int64_t inflight, int block,
+                     double electron_split) {
     if (!e) return global_err(OMC_E_ARG, "omc_event_params: null engine");
     cudaSetDevice(e->device);
-    return event_set_params(e, electron_tsteps, tail_boost, (long long)inflight, block);
+    return event_set_params(e, electron_tsteps, tail_boost, (long long)inflight, block, electron_split);
 }
 
 int omc_profile_last(const omc_engine *e, double *out, int n) {
@@ -689,17 +695,17 @@ int omc_replay(omc_engine *e, const double *prim, int nhist, const double *rn, c
     cudaSetDevice(e->device);
     long nrn = rn_off[nhist];
     long m = (long)nhist * dep_cap;
-    DBuf pd, rd, od, di, de, nd, nu, fl;
+    DBuf pd, rd, od, di, de, nd, nu, fl, sk;
     int rc;
     if ((rc = pd.alloc(nhist * 11 * 8)) || (rc = rd.alloc(std::max(1L, nrn) * 8)) || (rc = od.alloc((nhist + 1) * 8)) ||
         (rc = di.alloc(m * 4)) || (rc = de.alloc(m * 8)) || (rc = nd.alloc(nhist * 4)) || (rc = nu.alloc(nhist * 8)) ||
-        (rc = fl.alloc(nhist * 4)))
+        (rc = fl.alloc(nhist * 4)) || (rc = sk.alloc(plain_replay_stack_bytes(nhist))))
         return set_err(e, rc, "alloc");
     cudaMemcpyAsync(pd.p, prim, nhist * 11 * 8, cudaMemcpyHostToDevice, e->stream);
     if (nrn > 0) cudaMemcpyAsync(rd.p, rn, nrn * 8, cudaMemcpyHostToDevice, e->stream);
     cudaMemcpyAsync(od.p, rn_off, (nhist + 1) * 8, cudaMemcpyHostToDevice, e->stream);
     if ((rc = plain_replay(e, pd.as<double>(), nhist, rd.as<double>(), od.as<long>(), dep_cap, di.as<int>(),
-                           de.as<double>(), nd.as<int>(), nu.as<long>(), fl.as<unsigned>())))
+                           de.as<double>(), nd.as<int>(), nu.as<long>(), fl.as<unsigned>(), sk.p)))
         return rc;
     cudaMemcpyAsync(dep_ir, di.p, m * 4, cudaMemcpyDeviceToHost, e->stream);
     cudaMemcpyAsync(dep_e, de.p, m * 8, cudaMemcpyDeviceToHost, e->stream);

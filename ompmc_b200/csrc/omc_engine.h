@@ -97,6 +97,9 @@ int plain_beamlet_batch(omc_engine *e, const BeamletSrc<double> &S, int ib, doub
                         long n, int block);
 int plain_trace(omc_engine *e, const double *rays_d, int nrays, int cap, double *ustep, int *irnew, int *idisc,
                 int *ncalls, double *hn);
+// `stacks`: plain_replay_stack_bytes(nhist) of device memory for the
+// histories' particle stacks.
+size_t plain_replay_stack_bytes(int nhist);
 int plain_replay(omc_engine *e, const double *prim, int nhist, const double *rn, const long *rn_off, int dep_cap,
-                 int *dep_ir, double *dep_e, int *ndep, long *nused, unsigned *flags);
+                 int *dep_ir, double *dep_e, int *ndep, long *nused, unsigned *flags, void *stacks);
 }  // namespace omc

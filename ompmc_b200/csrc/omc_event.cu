@@ -31,6 +31,7 @@ namespace omc {
 
 constexpr int EV_BUDGET = 200000;  // transport steps one event may take
 constexpr int EV_MAXOUT = 1;       // secondaries an event emits: every interaction sampler pushes one
+constexpr int EV_MAXOUT_SPLIT = 2; // products of a split photon's sub-photon (pair: two)
 constexpr int EV_MAX_BLOCK = 256;  // launch bound of the transport kernels
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -39,13 +40,14 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
+template <int MAXOUT>
 struct EvEnv {
     Philox<float> rng;
     double *tally;
     int pend_ir;
     double pend_e;
-    Part<float> out[EV_MAXOUT];
-    uint32_t out_pos[EV_MAXOUT];  // parent's stream position at each push
+    Part<float> out[MAXOUT];
+    uint32_t out_pos[MAXOUT];     // parent's stream position at each push
     int nout;
     unsigned flags;
     int work;
@@ -72,12 +74,18 @@ struct EvEnv {
     __device__ void cross() { ncross++; }
     __device__ bool tstep_take() { return tleft-- > 0; }
     __device__ bool push(const Part<float> &q) {
-        if (nout >= EV_MAXOUT) {
+        if (nout >= MAXOUT) {
             flags |= ERR_STACK;
             return false;
         }
-        out_pos[nout] = rng.position();
-        out[nout++] = q;
+        // static indices keep the outputs in registers
+#pragma unroll
+        for (int k = 0; k < MAXOUT; k++)
+            if (k == nout) {
+                out_pos[k] = rng.position();
+                out[k] = q;
+            }
+        nout++;
         return true;
     }
     __device__ void err(unsigned f) { flags |= f; }
@@ -100,47 +108,75 @@ __device__ __forceinline__ void qload(const Queue &q, int i, Part<float> &p, int
     k0 = q.k0[i]; k1 = q.k1[i]; ctr = q.ctr[i];
 }
 
+// sp/sr: splitting state, stored where the queue has it (photon queues of
+// splitting engines); -1 = a photon not yet split.
 __device__ __forceinline__ void qstore(const Queue &q, int i, const Part<float> &p, int slot, uint32_t k0, uint32_t k1,
-                                       uint32_t ctr) {
+                                       uint32_t ctr, int sp = -1, float sr = 0.f) {
     q.x[i] = p.x; q.y[i] = p.y; q.z[i] = p.z;
     q.u[i] = p.u; q.v[i] = p.v; q.w[i] = p.w;
     q.e[i] = p.e; q.wt[i] = p.wt;
     q.ir[i] = p.ir;
     q.tag[i] = (p.iq + 1) | (slot << 2);
     q.k0[i] = k0; q.k1[i] = k1; q.ctr[i] = ctr;
+    if (q.sp) {
+        q.sp[i] = sp;
+        q.sr[i] = sr;
+    }
 }
 
-// Slot of a warp-aggregated append to `q` for the lanes with `want`;
-// -1 for the others (or on overflow, flagged).
-__device__ __forceinline__ int warp_append(const Queue &q, bool want, unsigned active, unsigned &flags) {
-    unsigned m = __ballot_sync(active, want);
-    if (!m) return -1;
-    int lane = threadIdx.x & 31;
-    int leader = __ffs(m) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(q.count, __popc(m));
-    base = __shfl_sync(active, base, leader);
+// Slot of a warp-aggregated append to `q` for the lanes with `want`: from
+// the bottom, or from the top for lanes with `hi`; -1 for the other lanes
+// (or on overflow, flagged).
+__device__ __forceinline__ int warp_append(const Queue &q, bool want, bool hi, unsigned active, unsigned &flags) {
+    const int lane = threadIdx.x & 31;
+    const unsigned mlo = __ballot_sync(active, want && !hi);
+    const unsigned mhi = __ballot_sync(active, want && hi);
+    int blo = 0, bhi = 0;
+    if (mlo) {
+        int leader = __ffs(mlo) - 1;
+        if (lane == leader) blo = atomicAdd(q.count, __popc(mlo));
+        blo = __shfl_sync(active, blo, leader);
+    }
+    if (mhi) {
+        int leader = __ffs(mhi) - 1;
+        if (lane == leader) bhi = atomicAdd(q.count_hi, __popc(mhi));
+        bhi = __shfl_sync(active, bhi, leader);
+    }
     if (!want) return -1;
-    int idx = base + __popc(m & lanemask_lt());
-    if (idx >= q.cap) {
+    int k = hi ? bhi + __popc(mhi & lanemask_lt()) : blo + __popc(mlo & lanemask_lt());
+    if (k >= q.cap) {
         flags |= ERR_QUEUE;
         return -1;
     }
-    return idx;
+    return hi ? q.cap - 1 - k : k;
+}
+
+// Entries of a queue (both ends) and the index of the f-th, top end first.
+__device__ __forceinline__ int queue_size(const Queue &q) {
+    return min(min(*q.count, q.cap) + min(*q.count_hi, q.cap), q.cap);
+}
+__device__ __forceinline__ int queue_index(const Queue &q, int f) {
+    int nhi = min(*q.count_hi, q.cap);
+    return f < nhi ? q.cap - 1 - f : f - nhi;
 }
 
 // Route the event's surviving particle and its secondaries to the output
-// queues.  A secondary's stream key is derived from its parent's key and
-// the parent's stream position when it was created.  All 32 lanes of the
-// warp take part (lanes without a particle pass alive = false, nout = 0).
-// Returns the particles this lane queued.
+// queues.  A secondary's stream key is derived from its parent's key, the
+// parent's stream position when it was created and its index among the
+// event's secondaries.  All 32 lanes of the warp take part (lanes without a
+// particle pass alive = false, nout = 0).  The survivor keeps its splitting
+// state (sp, sr); secondaries start unsplit.  Photons of zero weight (lost
+// a Russian roulette) would deposit nothing and are not queued.  Returns
+// the particles this lane queued.
+template <int MAXOUT>
 __device__ __forceinline__ int emit(const Queue &outP, const Queue &outE, bool alive, const Part<float> &p,
-                                    EvEnv &g, int slot, uint32_t k0, uint32_t k1) {
+                                    EvEnv<MAXOUT> &g, int slot, uint32_t k0, uint32_t k1, float esplit,
+                                    int sp = -1, float sr = 0.f) {
     const unsigned full = 0xffffffffu;
     uint64_t pkey = ((uint64_t)k1 << 32) | k0;
     int queued = 0;
 #pragma unroll
-    for (int k = 0; k < 1 + EV_MAXOUT; k++) {
+    for (int k = 0; k < 1 + MAXOUT; k++) {
         bool has;
         Part<float> q;
         uint32_t a0 = k0, a1 = k1, ac;
@@ -151,7 +187,8 @@ __device__ __forceinline__ int emit(const Queue &outP, const Queue &outE, bool a
         } else {
             has = k - 1 < g.nout;
             q = g.out[k - 1];
-            uint64_t ck = mix64(pkey * 0x9E3779B97F4A7C15ull + ((uint64_t)g.out_pos[k - 1] << 1) + 1u);
+            uint64_t ck = mix64(pkey * 0x9E3779B97F4A7C15ull + ((uint64_t)g.out_pos[k - 1] << 1) + 1u +
+                                ((uint64_t)(k - 1) << 40));
             a0 = (uint32_t)ck;
             a1 = (uint32_t)(ck >> 32);
             ac = 0;
@@ -161,11 +198,12 @@ __device__ __forceinline__ int emit(const Queue &outP, const Queue &outE, bool a
             g.flags |= ERR_NAN;
             has = false;
         }
+        if (has && q.iq == 0 && q.wt == 0.f) has = false;
         bool isph = has && q.iq == 0;
         bool isel = has && q.iq != 0;
-        int ip = warp_append(outP, isph, full, g.flags);
-        int ie = warp_append(outE, isel, full, g.flags);
-        if (ip >= 0) qstore(outP, ip, q, slot, a0, a1, ac);
+        int ip = warp_append(outP, isph, false, full, g.flags);
+        int ie = warp_append(outE, isel, esplit > 0.f && q.e > esplit, full, g.flags);
+        if (ip >= 0) qstore(outP, ip, q, slot, a0, a1, ac, k == 0 ? sp : -1, k == 0 ? sr : 0.f);
         if (ie >= 0) qstore(outE, ie, q, slot, a0, a1, ac);
         queued += (ip >= 0) + (ie >= 0);
     }
@@ -192,16 +230,84 @@ __device__ __forceinline__ void add_live(int *live, int nbmax, int slot, int del
     if (tot != 0 && (threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&live[req], tot);
 }
 
+// One event of a split photon (photon splitting, ompmc.c:1867-2139 with
+// nsplit > 1).  A queued photon is a ray of nsplit sub-photons of weight
+// wt/nsplit whose interaction sites are stratified along it.  Its first
+// event checks the cut-off, draws the stratification offset r and the
+// surviving sub-photon, and sets the ray's weight; every event then moves
+// one sub-photon, k, from the previous site by its share of mean free
+// paths, ln(eta_{k-1} / eta_k) with eta_k = (nsplit - k - r) / nsplit
+// (eta_{-1} = 1), and samples its interaction.  The charged products are
+// pushed with the sub-photon's weight; the scattered photon of the
+// surviving sub-photon is pushed with the full weight (as a new, unsplit
+// photon) and the others' are dropped.  p becomes the ray at the site;
+// returns true while it has sub-photons left.  The draws differ from the
+// plain form's order (one stream per ray), the sampled distribution is the
+// same.
+template <typename Env>
+__device__ __forceinline__ bool split_event(const DevData<float> &D, Env &g, Part<float> &p, int &sp, float &sr) {
+    const int ns = D.nsplit;
+    if (sp < 0) {
+        if (p.e <= pcut_of(D, p.ir) || p.wt == 0.f) {
+            g.deposit(p.ir, p.wt * p.e);
+            return false;
+        }
+        sr = g.uni();
+        int isurv = (int)(g.uni() * (float)ns);
+        sp = min(isurv, ns - 1);
+        p.wt = p.wt / (float)ns;
+    }
+    const int isplit = sp >> 16, isurv = sp & 0xffff;
+    const float den = (float)(ns - isplit) - sr;
+    if (den <= 0.f) return false;
+    const float num = isplit == 0 ? (float)ns : den + 1.f;
+    const float dpmfp = m_log(num / den);
+    const float gle = m_log(p.e);
+    Part<float> q = p;
+    q.iq = 0;
+    int imed, lgle;
+    float cohfac;
+    if (!photon_walk(D, g, q, gle, dpmfp, imed, lgle, cohfac)) return false;
+    p.x = q.x; p.y = q.y; p.z = q.z;
+    p.ir = q.ir;
+    const bool surv = isplit == isurv;
+    if (g.uni() <= 1.f - cohfac) {
+        if (surv) {
+            q.wt *= (float)ns;
+            rayleigh(D, g, q, imed, gle, lgle);
+            g.push(q);
+        }
+    } else {
+        photon_interact(D, g, q, p.e, gle, imed, lgle);
+        // the interaction pushed at most one product; keep it and q as the
+        // splitting rules say
+        if (g.nout == 1 && g.out[0].iq == 0) {
+            if (surv) g.out[0].wt *= (float)ns;
+            else g.nout = 0;
+        }
+        if (q.iq != 0 || surv) {
+            if (q.iq == 0) q.wt *= (float)ns;
+            g.push(q);
+        }
+    }
+    sp = ((isplit + 1) << 16) | isurv;
+    return isplit + 1 < ns;
+}
+
 // Events of one queue.  Warps take 32 particles at a time from a counter,
 // so work is balanced between warps however long their events run.
-template <bool PHOTON>
+// KIND: EV_PHOTON, EV_ELECTRON, or EV_SPLIT (photons of a splitting engine).
+enum { EV_PHOTON = 0, EV_ELECTRON = 1, EV_SPLIT = 2 };
+template <int KIND>
 __device__ __forceinline__ void transport_events(const DevData<float> &D, const Queue &in, const Queue &outP,
                                                  const Queue &outE, double *tallies, long nvox, Ctl *ctl,
                                                  uint32_t seedw, int *live, int nbmax) {
+    constexpr int MAXOUT = KIND == EV_SPLIT ? EV_MAXOUT_SPLIT : EV_MAXOUT;
     const unsigned full = 0xffffffffu;
-    const int kq = PHOTON ? 0 : 1;
-    const int n = min(*in.count, in.cap);
+    const int kq = KIND == EV_ELECTRON ? 1 : 0;
+    const int n = queue_size(in);
     const int tsteps = ctl->tsteps;
+    const float esplit = ctl->esplit;
     const int lane = threadIdx.x & 31;
     unsigned flags = 0;
     unsigned c_ev = 0, c_steps = 0, c_cross = 0, c_dep = 0, c_atom = 0;
@@ -210,14 +316,20 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
         if (lane == 0) base = atomicAdd(&ctl->fetch[kq], 32);
         base = __shfl_sync(full, base, 0);
         if (base >= n) break;
-        const int i = base + lane;
-        const bool valid = i < n;
+        const bool valid = base + lane < n;
+        const int i = valid ? queue_index(in, base + lane) : 0;
         Part<float> p;
         int tag = 0;
         uint32_t k0 = 0, k1 = 0, pos = 0;
         if (valid) qload(in, i, p, tag, k0, k1, pos);
+        int sp = -1;
+        float sr = 0.f;
+        if (KIND == EV_SPLIT && valid) {
+            sp = in.sp[i];
+            sr = in.sr[i];
+        }
         const int slot = tag >> 2;
-        EvEnv g;
+        EvEnv<MAXOUT> g;
         g.rng.init(((uint64_t)k1 << 32) | k0, seedw, pos);
         g.tally = tallies + (long)slot * nvox;
         g.pend_ir = -1;
@@ -229,10 +341,12 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
         g.ncross = g.ndep = g.natom = 0;
         bool alive = false;
         if (valid) {
-            alive = PHOTON ? photon_step(D, g, p) : electron_step(D, g, p) == E_ALIVE;
+            if (KIND == EV_PHOTON) alive = photon_step(D, g, p);
+            else if (KIND == EV_ELECTRON) alive = electron_step(D, g, p) == E_ALIVE;
+            else alive = split_event(D, g, p, sp, sr);
             g.flush();
         }
-        int emitted = emit(outP, outE, alive, p, g, slot, k0, k1);
+        int emitted = emit(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr);
         if (live) add_live(live, nbmax, valid ? slot : 0, valid ? emitted - 1 : 0, full);
         flags |= g.flags;
         c_ev += valid;
@@ -254,7 +368,14 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
 __global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_step(DevData<float> D, Queue in, Queue outP, Queue outE,
                                                      double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
                                                      int *live, int nbmax) {
-    transport_events<true>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax);
+    transport_events<EV_PHOTON>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax);
+}
+
+// Photon events of a splitting engine (nsplit > 1): one sub-photon each.
+__global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_split_step(DevData<float> D, Queue in, Queue outP,
+                                                           Queue outE, double *tallies, long nvox, Ctl *ctl,
+                                                           uint32_t seedw, int *live, int nbmax) {
+    transport_events<EV_SPLIT>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax);
 }
 
 // Electron/positron events of the queued charged particles: at most the
@@ -263,7 +384,7 @@ __global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_step(DevData<float> D, 
 __global__ void __launch_bounds__(EV_MAX_BLOCK) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
                                                        double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
                                                        int *live, int nbmax) {
-    transport_events<false>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax);
+    transport_events<EV_ELECTRON>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax);
 }
 
 __global__ void k_source(DevData<float> D, BeamSrc<float> S, Queue qP, Queue qE, Ctl *ctl, long long nper,
@@ -282,8 +403,8 @@ __global__ void k_source(DevData<float> D, BeamSrc<float> S, Queue qP, Queue qE,
         Part<float> p = beam_primary(D, S, g, ein);
         es += ein;
         int slot = (int)(h / nper);
-        int ip = warp_append(qP, p.iq == 0, active, flags);
-        int ie = warp_append(qE, p.iq != 0, active, flags);
+        int ip = warp_append(qP, p.iq == 0, false, active, flags);
+        int ie = warp_append(qE, p.iq != 0, ctl->esplit > 0.f && p.e > ctl->esplit, active, flags);
         if (ip >= 0) qstore(qP, ip, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.position());
         if (ie >= 0) qstore(qE, ie, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.position());
     }
@@ -304,32 +425,47 @@ __device__ __forceinline__ void plan_budget(Ctl *ctl, long long nE, const PlanCf
         me = me > c.boost ? c.boost : me;
     }
     ctl->tsteps = (int)(c.tsteps * me);
+    ctl->esplit = c.esplit;
     ctl->fetch[0] = 0;
     ctl->fetch[1] = 0;
 }
 
-// Histories to inject this cycle: keep `target` particles in flight.  Also
+// Particles in the cycle's input queues; an overflow of either (the two
+// ends met) is flagged.  The output queues (the previous cycle's inputs,
+// all consumed) are emptied.
+__device__ __forceinline__ void plan_queues(Ctl *ctl, int iph, int iel, int cap, long long &np, long long &ne) {
+    np = (long long)ctl->cnt[iph] + ctl->cnt_hi[iph];
+    ne = (long long)ctl->cnt[iel] + ctl->cnt_hi[iel];
+    if (np > cap || ne > cap) ctl->flags |= ERR_QUEUE;
+    np = np > cap ? cap : np;
+    ne = ne > cap ? cap : ne;
+    ctl->cnt[iph ^ 2] = 0;
+    ctl->cnt[iel ^ 2] = 0;
+    ctl->cnt_hi[iph ^ 2] = 0;
+    ctl->cnt_hi[iel ^ 2] = 0;
+}
+
+// Histories to inject this cycle: keep `target` particles in flight (a
+// photon of a splitting engine counts nsplit times).  Also
 // sets the cycle's electron budget and empties the output queues (the
 // previous cycle's inputs, all consumed).
 __global__ void k_plan(Ctl *ctl, int iph, int iel, PlanCfg c) {
-    int oph = iph ^ 2, oel = iel ^ 2;
-    long long np = min(ctl->cnt[iph], c.cap), ne = min(ctl->cnt[iel], c.cap);
+    long long np, ne;
+    plan_queues(ctl, iph, iel, c.cap, np, ne);
     long long rem = ctl->hist_total - ctl->hist_next;
-    long long inj = c.target - (np + ne);
+    long long inj = (c.target - (np * c.pweight + ne)) / c.pweight;
     if (inj < 0) inj = 0;
     if (inj > rem) inj = rem;
-    long long room = (long long)c.cap - ctl->cnt[iph];
+    long long room = (long long)c.cap - (np > ne ? np : ne);
     if (inj > room) inj = room > 0 ? room : 0;
     ctl->inject = (int)inj;
     ctl->hist_base = ctl->hist_next;
     ctl->hist_next += inj;
-    ctl->cnt[oph] = 0;
-    ctl->cnt[oel] = 0;
     plan_budget(ctl, ne, c);
 }
 
 // ------------------------------------------------------------------ host
-static int alloc_queue(omc_engine *e, DBuf &b, Queue &q, int cap, int *count) {
+static int alloc_queue(omc_engine *e, DBuf &b, Queue &q, int cap, int *count, int *count_hi) {
     size_t per = (size_t)cap * 4;
     int rc = b.alloc(per * 13);
     if (rc) return set_err(e, rc, "event queue allocation failed");
@@ -342,8 +478,28 @@ static int alloc_queue(omc_engine *e, DBuf &b, Queue &q, int cap, int *count) {
     q.k1 = (uint32_t *)(p + per * 11);
     q.ctr = (uint32_t *)(p + per * 12);
     q.count = count;
+    q.count_hi = count_hi;
     q.cap = cap;
+    q.sp = nullptr;
+    q.sr = nullptr;
     return OMC_OK;
+}
+
+using TransportKernel = void (*)(DevData<float>, Queue, Queue, Queue, double *, long, Ctl *, uint32_t, int *, int);
+
+// The photon kernel of the engine: split photons when nsplit > 1.
+static TransportKernel photon_kernel(const omc_engine *e) {
+    return e->d32.d.nsplit > 1 ? k_photon_split_step : k_photon_step;
+}
+
+// Resident blocks per SM of the transport kernels -> one-wave grids.
+static void size_grids(omc_engine *e, EventState &S) {
+    int bp = 0, be = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, photon_kernel(e), S.block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, k_electron_step, S.block, 0);
+    S.grid_p = e->sm_count * std::max(1, bp);
+    S.grid_e = e->sm_count * std::max(1, be);
+    S.lanes = S.grid_e * S.block;
 }
 
 int event_prepare(omc_engine *e) {
@@ -356,31 +512,38 @@ int event_prepare(omc_engine *e) {
     // most the transport kernels' launch bound
     S.block = e->opt.block > 0 ? std::min(EV_MAX_BLOCK, (e->opt.block + 31) / 32 * 32) : 256;
     S.grid = e->sm_count * std::max(1, 2048 / S.block);
-    int bp = 0, be = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_photon_step, S.block, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, k_electron_step, S.block, 0);
-    S.grid_p = e->sm_count * std::max(1, bp);
-    S.grid_e = e->sm_count * std::max(1, be);
-    S.lanes = S.grid_e * S.block;
+    size_grids(e, S);
     // 2 measured best on the slab workload while the queues are full
     S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 2;
     S.boost = e->opt.tail_boost > 0 ? e->opt.tail_boost : 32;
     S.inflight = e->opt.inflight > 0 ? e->opt.inflight : (1LL << 20);
+    S.esplit = e->opt.electron_split > 0 ? e->opt.electron_split + D_RM : 0.0;
     int rc = S.ctl.alloc(sizeof(Ctl));
     if (rc) return set_err(e, rc, "control block allocation failed");
     S.ctl_d = S.ctl.as<Ctl>();
     for (int i = 0; i < 4; i++)
-        if ((rc = alloc_queue(e, S.buf[i], S.q[i], S.cap, &S.ctl_d->cnt[i]))) return rc;
+        if ((rc = alloc_queue(e, S.buf[i], S.q[i], S.cap, &S.ctl_d->cnt[i], &S.ctl_d->cnt_hi[i]))) return rc;
+    if (e->d32.d.nsplit > 1) {
+        // splitting state of the two photon queues (A and B)
+        for (int k = 0; k < 2; k++) {
+            size_t per = (size_t)S.cap * 4;
+            if ((rc = S.split_buf[k].alloc(per * 2))) return set_err(e, rc, "splitting state allocation failed");
+            Queue &q = S.q[2 * k];
+            q.sp = S.split_buf[k].as<int>();
+            q.sr = (float *)((char *)S.split_buf[k].p + per);
+        }
+    }
     S.ready = true;
     return OMC_OK;
 }
 
 // Event-form tuning parameters of an engine (values <= 0 keep the current
 // one); the queues are not reallocated.
-int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, int block) {
+int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, int block, double split_kinetic) {
     if (tsteps > 0) e->opt.electron_tsteps = tsteps;
     if (boost > 0) e->opt.tail_boost = boost;
     if (inflight > 0) e->opt.inflight = inflight;
+    if (split_kinetic >= 0) e->opt.electron_split = split_kinetic;
     if (block > 0) {
         if (block % 32 || block > EV_MAX_BLOCK)
             return set_err(e, OMC_E_ARG, "block must be a multiple of 32, at most 256");
@@ -391,14 +554,10 @@ int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, i
         S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 2;
         S.boost = e->opt.tail_boost > 0 ? e->opt.tail_boost : 32;
         S.inflight = e->opt.inflight > 0 ? e->opt.inflight : (1LL << 20);
+        S.esplit = e->opt.electron_split > 0 ? e->opt.electron_split + D_RM : 0.0;
         S.block = e->opt.block > 0 ? std::min(EV_MAX_BLOCK, e->opt.block) : 256;
         S.grid = e->sm_count * std::max(1, 2048 / S.block);
-        int bp = 0, be = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_photon_step, S.block, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, k_electron_step, S.block, 0);
-        S.grid_p = e->sm_count * std::max(1, bp);
-        S.grid_e = e->sm_count * std::max(1, be);
-        S.lanes = S.grid_e * S.block;
+        size_grids(e, S);
     }
     return OMC_OK;
 }
@@ -411,6 +570,8 @@ PlanCfg plan_cfg(const omc_engine *e, long long target) {
     c.lanes = S.lanes;
     c.boost = S.boost;
     c.tsteps = S.tsteps;
+    c.esplit = (float)S.esplit;
+    c.pweight = std::max(1, e->d32.d.nsplit);
     return c;
 }
 
@@ -433,7 +594,7 @@ static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, doubl
     if (ev) cudaEventRecord(ev[1], e->stream);
     k_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, src, S.q[iph], S.q[iel], S.ctl_d, nper, seed, seedw);
     if (ev) cudaEventRecord(ev[2], e->stream);
-    k_photon_step<<<S.grid_p, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
+    photon_kernel(e)<<<S.grid_p, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
                                                             S.ctl_d, seedw, nullptr, 1);
     if (ev) cudaEventRecord(ev[3], e->stream);
     k_electron_step<<<S.grid_e, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
@@ -465,8 +626,8 @@ static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallie
         int oph = in == 0 ? 2 : 0;
         double row[6] = {(double)h.inject, (double)cnt_in[0] + h.inject, (double)cnt_in[1], t[1], t[2], t[3]};
         S.trace.insert(S.trace.end(), row, row + 6);
-        cnt_in[0] = std::min(h.cnt[oph], S.cap);
-        cnt_in[1] = std::min(h.cnt[oph + 1], S.cap);
+        cnt_in[0] = std::min(h.cnt[oph] + h.cnt_hi[oph], S.cap);
+        cnt_in[1] = std::min(h.cnt[oph + 1] + h.cnt_hi[oph + 1], S.cap);
         S.prof[3].seconds += t[0] * 1e-3;
         S.prof[3].launches += 1;
         S.prof[0].seconds += t[1] * 1e-3;
@@ -567,7 +728,9 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
         cudaMemcpyAsync(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost, e->stream);
         if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "event transport"))) break;
         // a graph ends with a B -> A cycle: its outputs are queues A
-        if (h.hist_next >= h.hist_total && h.cnt[0] == 0 && h.cnt[1] == 0) break;
+        if (h.hist_next >= h.hist_total && h.cnt[0] == 0 && h.cnt[1] == 0 && h.cnt_hi[0] == 0 &&
+            h.cnt_hi[1] == 0)
+            break;
         if (h.flags & ERR_QUEUE) break;
         // every cycle advances each queued particle by one event, so a run
         // needs (histories / injection rate) + (longest history) cycles
@@ -602,9 +765,10 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
 // first served, keeping `target` particles in flight.
 __global__ void k_serve_plan(ServeDev *sd, Ctl *ctl, int iph, int iel, PlanCfg c) {
     const int cap = c.cap;
-    long long np = min(ctl->cnt[iph], cap), ne = min(ctl->cnt[iel], cap);
-    long long room = c.target - (np + ne);
-    long long qroom = (long long)cap - max(ctl->cnt[iph], ctl->cnt[iel]);
+    long long np, ne;
+    plan_queues(ctl, iph, iel, cap, np, ne);
+    long long room = (c.target - (np * c.pweight + ne)) / c.pweight;
+    long long qroom = (long long)cap - (np > ne ? np : ne);
     if (room > qroom) room = qroom;
     int nplan = 0;
     long long cum = 0;
@@ -625,8 +789,6 @@ __global__ void k_serve_plan(ServeDev *sd, Ctl *ctl, int iph, int iel, PlanCfg c
     sd->plan_cum[nplan] = (int)cum;
     sd->nplan = nplan;
     sd->inject_total = (int)cum;
-    ctl->cnt[iph ^ 2] = 0;
-    ctl->cnt[iel ^ 2] = 0;
     plan_budget(ctl, ne, c);
 }
 
@@ -653,8 +815,8 @@ __global__ void k_serve_source(DevData<float> D, ServeDev *sd, Queue qP, Queue q
         float ein;
         Part<float> p = r.kind == 0 ? beam_primary(D, sd->beam[s], g, ein) : beamlet_primary(D, sd->bl[s], r.bixel, g, ein);
         int slot = s * nbmax + (int)(local / r.nper);
-        int ip = warp_append(qP, p.iq == 0, active, flags);
-        int ie = warp_append(qE, p.iq != 0, active, flags);
+        int ip = warp_append(qP, p.iq == 0, false, active, flags);
+        int ie = warp_append(qE, p.iq != 0, ctl->esplit > 0.f && p.e > ctl->esplit, active, flags);
         if (ip >= 0) qstore(qP, ip, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.position());
         if (ie >= 0) qstore(qE, ie, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.position());
         add_live(sd->live, nbmax, slot, (ip >= 0) + (ie >= 0), active);
@@ -671,7 +833,7 @@ void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, in
     long nvox = e->ph.nvox();
     k_serve_plan<<<1, 1, 0, e->stream>>>(sd, S.ctl_d, iph, iel, plan_cfg(e, target));
     k_serve_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, sd, S.q[iph], S.q[iel], S.ctl_d, nbmax, seedw);
-    k_photon_step<<<S.grid_p, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
+    photon_kernel(e)<<<S.grid_p, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
                                                         S.ctl_d, seedw, sd->live, nbmax);
     k_electron_step<<<S.grid_e, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
                                                           S.ctl_d, seedw, sd->live, nbmax);

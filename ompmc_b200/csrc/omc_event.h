@@ -8,17 +8,28 @@ namespace omc {
 // Structure-of-arrays particle queue in device memory.  `tag` packs the
 // charge (iq+1, 2 bits) and the tally slot (upper bits); k0/k1 are the
 // particle's Philox stream key and ctr its stream position (numbers drawn).
+// Entries fill from both ends: `count` entries from index 0 up and
+// `count_hi` entries from index cap-1 down (electron queues put particles
+// above the regroup energy at the top, so that warps see particles of one
+// kind).
 struct Queue {
     float *x, *y, *z, *u, *v, *w, *e, *wt;
     int *ir, *tag;
     uint32_t *k0, *k1, *ctr;
-    int *count;      // device counter of occupied entries
+    // photon splitting state (photon queues of engines with nsplit > 1,
+    // else null): -1 for a photon not yet split, else (next sub-photon << 16)
+    // | surviving sub-photon; and the ray's stratification offset
+    int *sp;
+    float *sr;
+    int *count;      // device counter of entries from the bottom
+    int *count_hi;   // device counter of entries from the top
     int cap;
 };
 
 // Cycle control block in device memory.
 struct Ctl {
-    int cnt[4];               // photon A, electron A, photon B, electron B
+    int cnt[4];               // photon A, electron A, photon B, electron B (from the bottom)
+    int cnt_hi[4];            // the same queues, entries from the top
     long long hist_next;      // next history to inject
     long long hist_total;     // histories requested
     int inject;               // histories injected this cycle
@@ -28,7 +39,7 @@ struct Ctl {
     int pad;
     double src_energy;        // sum of primary kinetic energies
     int tsteps;               // this cycle's electron budget (tstep-loop iterations per event)
-    int pad2;
+    float esplit;             // regroup energy (total, MeV): electrons above it go to the top
     int fetch[2];             // work counters of the photon and electron kernels
     // counters per transport kernel (0 photon, 1 electron)
     unsigned long long st_events[2], st_steps[2], st_cross[2], st_dep[2], st_atom[2];
@@ -46,12 +57,16 @@ struct PlanCfg {
     int lanes;                // resident threads of the transport kernels
     int boost;                // largest budget multiplier as the queues drain (1 = fixed)
     int tsteps;               // base electron budget (tstep-loop iterations)
+    float esplit;             // regroup energy of the electron queues (total, MeV; 0 = one group)
+    int pweight;              // in-flight weight of a queued photon: nsplit (each makes up to
+                              // nsplit charged particles), 1 without splitting
 };
 
 struct EventState {
     bool ready = false;
     int cap = 0;              // per queue
     DBuf buf[4];              // photon A, electron A, photon B, electron B (13 arrays each)
+    DBuf split_buf[2];        // splitting state of the photon queues (nsplit > 1)
     Queue q[4];
     DBuf ctl;
     Ctl *ctl_d = nullptr;
@@ -61,6 +76,7 @@ struct EventState {
     int lanes = 0;            // resident threads of the electron kernel
     int boost = 32;           // budget multiplier limit in the drain tail
     int tsteps = 2;           // electron tstep iterations per event launch
+    double esplit = 0;        // regroup energy of the electron queues (total, MeV)
     long long inflight = 0;   // particles kept in flight by the injector
     KernelProfile prof[4];    // 0 source, 1 photon, 2 electron, 3 plan+reset
     // profiled runs: per cycle {histories injected, photons in, electrons in,
@@ -101,7 +117,7 @@ int event_prepare(omc_engine *e);
 // particle = request slot * nbmax + batch.
 void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
 PlanCfg plan_cfg(const omc_engine *e, long long target);
-int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, int block);
+int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, int block, double split_kinetic);
 
 int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint64_t seed, double *sum, double *sum2,
                    double *src_energy, KernelStats &ks);

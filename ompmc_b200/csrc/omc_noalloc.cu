@@ -73,6 +73,8 @@ extern "C" int omc_run_beam_noalloc(omc_engine *e, const omc_beam *b, int64_t nc
     if (nbatch < 2) return set_err(e, OMC_E_ARG, "nbatch must be >= 2 for the batch uncertainty");
     if (b->energy.n > 0 && (!b->energy.cdf1 || !b->energy.cdf2)) return set_err(e, OMC_E_ARG, "spectrum arrays missing");
     if (b->energy.charge < -1 || b->energy.charge > 1) return set_err(e, OMC_E_ARG, "charge must be -1, 0 or 1");
+    if (e->opt.nsplit > 1)
+        return set_err(e, OMC_E_RANGE, "omc_run_beam_noalloc: photon splitting (nsplit > 1) needs omc_run_beam");
     long nv = e->ph.nvox();
     if (nv > MAXV)
         return set_err(e, OMC_E_RANGE,

@@ -501,27 +501,18 @@ OMC_COLD void photo(const DevData<R> &D, Env &g, Part<R> &p) {
 }
 
 // --------------------------------------------------------- photon step
-// One call of photon(): cut-off check, number of mean free paths, voxel
-// walk to the interaction site and the interaction (photon, ompmc.c:1867-2139
-// with nsplit = 1).  Returns false when the photon is gone.
+// Voxel walk of a photon to its interaction site `dpmfp` mean free paths
+// ahead (the transport loop of photon, ompmc.c:1957-2037).  Returns false
+// when the photon leaves the geometry (or a guard trips); otherwise p is at
+// the site and imed, lgle and cohfac are those of the site's medium.
 template <typename R, typename Env>
-OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
-    R eig = p.e;
+OMC_HD bool photon_walk(const DevData<R> &D, Env &g, Part<R> &p, R gle, R dpmfp, int &imed, int &lgle, R &cohfac) {
     int irl = p.ir;
-    if (eig <= pcut_of(D, irl) || p.wt == R(0)) {
-        g.deposit(irl, p.wt * eig);
-        return false;
-    }
-    R gle = m_log(eig);
-    // nsplit = 1: the mean-free-path draw and the survivor draw
-    R rnno = g.uni();
-    R eta_prime = (R(1) - rnno + R(1)) - R(1);
-    (void)g.uni();
-    R dpmfp = -m_log(eta_prime);
     int irold = irl;
-    int imed = D.med[irl];
-    int lgle = 0;
-    R gmfp = 0, cohfac = 0;
+    imed = D.med[irl];
+    lgle = 0;
+    cohfac = 0;
+    R gmfp = 0;
     int guard = 0;
     for (;;) {
         R tstep;
@@ -552,15 +543,18 @@ OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
             imed = D.med[irl];
             g.cross();
         }
-        if (imed != -1 && dpmfp <= R(1.0E-5)) break;
+        if (imed != -1 && dpmfp <= R(1.0E-5)) return true;
         if (++guard > 100000 || !g.tick()) { g.err(ERR_LOOP); return false; }
     }
-    rnno = g.uni();
-    if (rnno <= R(1) - cohfac) {
-        rayleigh(D, g, p, imed, gle, lgle);
-        return true;
-    }
-    rnno = g.uni();
+}
+
+// The interaction at the end of a walk, after the Rayleigh draw came out
+// against Rayleigh: pair, Compton or photo-absorption by the branching
+// ratios of the site (ompmc.c:2060-2085).  p becomes the interaction's
+// first product; a second one, if any, is pushed.
+template <typename R, typename Env>
+OMC_HD void photon_interact(const DevData<R> &D, Env &g, Part<R> &p, R eig, R gle, int imed, int lgle) {
+    R rnno = g.uni();
     const PhBin<R> &b = pbin(D, imed, lgle);
     R gbr1 = pwl(b.gbr1, gle);
     if (rnno <= gbr1 && eig > R(2) * R(D_RM)) {
@@ -570,7 +564,50 @@ OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
         if (rnno < gbr2) compton(D, g, p);
         else photo(D, g, p);
     }
+}
+
+// One call of photon(): cut-off check, number of mean free paths, voxel
+// walk to the interaction site and the interaction (photon, ompmc.c:1867-2139
+// with nsplit = 1).  Returns false when the photon is gone.
+template <typename R, typename Env>
+OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
+    R eig = p.e;
+    int irl = p.ir;
+    if (eig <= pcut_of(D, irl) || p.wt == R(0)) {
+        g.deposit(irl, p.wt * eig);
+        return false;
+    }
+    R gle = m_log(eig);
+    // nsplit = 1: the mean-free-path draw and the survivor draw
+    R rnno = g.uni();
+    R eta_prime = (R(1) - rnno + R(1)) - R(1);
+    (void)g.uni();
+    R dpmfp = -m_log(eta_prime);
+    int imed, lgle;
+    R cohfac;
+    if (!photon_walk(D, g, p, gle, dpmfp, imed, lgle, cohfac)) return false;
+    rnno = g.uni();
+    if (rnno <= R(1) - cohfac) {
+        rayleigh(D, g, p, imed, gle, lgle);
+        return true;
+    }
+    photon_interact(D, g, p, eig, gle, imed, lgle);
     return true;
+}
+
+// Russian roulette of a photon made by an electron interaction when photons
+// are split (ompmc.c:4169-4182, 4358-4371, 4647-4660): it survives with
+// probability 1/nsplit and then carries nsplit times its weight; otherwise
+// its weight and energy are zeroed (it deposits nothing).
+template <typename R, typename Env>
+OMC_HD void roulette(const DevData<R> &D, Env &g, Part<R> &q) {
+    R rnno = g.uni();
+    if (rnno * R(D.nsplit) > R(1)) {
+        q.wt = R(0);
+        q.e = R(0);
+    } else {
+        q.wt *= R(D.nsplit);
+    }
 }
 
 // ---------------------------------------------- electron samplers (e+-)
@@ -593,6 +630,10 @@ OMC_COLD void rannih(const DevData<R> &D, Env &g, Part<R> &p) {
     q.u = -p.u;
     q.v = -p.v;
     q.w = -p.w;
+    if (D.nsplit > 1) {
+        roulette(D, g, p);
+        roulette(D, g, q);
+    }
     g.push(q);
 }
 
@@ -688,6 +729,7 @@ OMC_COLD void brems(const DevData<R> &D, Env &g, Part<R> &p) {
         q.w = c * costhe;
     }
     p.e = ese;
+    if (D.nsplit > 1) roulette(D, g, q);
     g.push(q);
 }
 
@@ -825,6 +867,10 @@ OMC_COLD void annih(const DevData<R> &D, Env &g, Part<R> &p) {
     costhe = m_min(R(1), (esg2 - RMr) * pot / esg2);
     sinthe = -m_sqrt(R(1) - costhe * costhe);
     dir(costhe, sinthe, q.u, q.v, q.w);
+    if (D.nsplit > 1) {
+        roulette(D, g, p);
+        roulette(D, g, q);
+    }
     g.push(q);
 }
 

@@ -13,6 +13,10 @@
 namespace omc {
 
 constexpr int PLAIN_STACK = 48;
+// Stack of the kernels used when photons are split: each split photon
+// leaves up to about nsplit charged particles below its survivor, so the
+// depth grows by about nsplit per photon generation (nsplit <= 64).
+constexpr int SPLIT_STACK = 256;
 // Transport steps (photon voxel steps + electron CH steps) one history may
 // take before it is stopped with ERR_LOOP; typical histories take < 1e3.
 constexpr long HISTORY_BUDGET = 2000000;
@@ -22,6 +26,7 @@ struct PlainEnv {
     Rng rng;
     double *endep;       // per-voxel energy tally of the batch (index ir-1)
     Part<double> *st;    // the history's stack
+    int cap;             // its capacity
     int top;             // slot of the particle being processed
     int nchild;          // particles pushed above it
     unsigned flags;
@@ -33,7 +38,7 @@ struct PlainEnv {
     }
     __device__ bool push(const Part<double> &q) {
         int slot = top + 1 + nchild;
-        if (slot >= PLAIN_STACK) {
+        if (slot >= cap) {
             flags |= ERR_STACK;
             return false;
         }
@@ -44,7 +49,133 @@ struct PlainEnv {
     __device__ void err(unsigned f) { flags |= f; }
     __device__ void cross() {}
     __device__ bool tstep_take() const { return true; }
+    // the split photon's survivor is moved below its charged products
+    static constexpr bool kRefOrder = false;
 };
+
+// Stack of the replay kernel (global memory, one per history): splitting
+// in the reference's stack order leaves about nsplit/2 charged particles
+// below each generation's surviving photon.
+constexpr int REPLAY_STACK = 4096;
+
+// photon() with photon splitting (ompmc.c:1867-2139, nsplit > 1) for the
+// photon on top of the stack (slot np); returns the new top slot.  The
+// photon is split into nsplit sub-photons of weight wt/nsplit whose
+// interaction sites are stratified along its ray: sub-photon k travels
+// -ln(eta_k) - sum of the previous ones' mean free paths from the previous
+// site, with eta_k = 1 - (r + k)/nsplit.  Every sub-photon's charged
+// products are kept; the scattered photon of one sub-photon, drawn at the
+// start, survives with the full weight and the others' are removed.  Once
+// the loop ends a photon on top of the stack is split again at once.
+template <typename Env>
+__device__ int photon_split(const DevData<double> &D, Env &g, Part<double> *st, int np) {
+    const int ns = D.nsplit;
+    double eig = st[np].e;
+    int irl = st[np].ir;
+    if (eig <= pcut_of(D, irl) || st[np].wt == 0.0) {
+        g.deposit(irl, st[np].wt * eig);
+        return np - 1;
+    }
+    double gle = log(eig);
+    for (int resplit = 0;; resplit++) {
+        if (resplit > 100000) {
+            g.err(ERR_LOOP);
+            return -1;
+        }
+        double rnno = g.uni();
+        rnno /= (double)ns;
+        const double d_eta = 1.0 / (double)ns;
+        double eta_prime = 1.0 - rnno + d_eta;
+        Part<double> save = st[np];
+        const double wtsave = save.wt / (double)ns;
+        const int s0 = np;
+        np -= 1;
+        rnno = g.uni();
+        const int isurv = (int)(rnno * ns);
+        double dpmfp_old = 0.0;
+        for (int isplit = 0; isplit < ns; isplit++) {
+            eta_prime -= d_eta;
+            if (eta_prime <= 0.0) break;
+            double dpmfp = -log(eta_prime) - dpmfp_old;
+            dpmfp_old += dpmfp;
+            np += 1;
+            if (np >= g.cap) {
+                g.err(ERR_STACK);
+                return -1;
+            }
+            Part<double> q = save;
+            q.wt = wtsave;
+            q.iq = 0;
+            int imed, lgle;
+            double cohfac;
+            if (!photon_walk(D, g, q, gle, dpmfp, imed, lgle, cohfac)) {
+                np -= 1;     // discarded: the rest of the ray lies beyond it
+                break;
+            }
+            save.x = q.x; save.y = q.y; save.z = q.z;
+            save.ir = q.ir;
+            rnno = g.uni();
+            if (rnno <= 1.0 - cohfac) {
+                if (isplit != isurv) {
+                    np -= 1;
+                } else {
+                    q.wt *= ns;
+                    rayleigh(D, g, q, imed, gle, lgle);
+                    st[np] = q;
+                }
+                continue;
+            }
+            g.top = np;
+            g.nchild = 0;
+            photon_interact(D, g, q, eig, gle, imed, lgle);
+            st[np] = q;
+            int ip = np;
+            np += g.nchild;
+            // the non-surviving sub-photons' scattered photons leave the
+            // stack: the top entry moves into the freed slot (all products
+            // of the interaction share its position and region)
+            do {
+                if (st[ip].iq == 0) {
+                    if (isplit != isurv) {
+                        if (ip < np) {
+                            st[ip].e = st[np].e; st[ip].iq = st[np].iq;
+                            st[ip].u = st[np].u; st[ip].v = st[np].v; st[ip].w = st[np].w;
+                            st[ip].wt = st[np].wt;
+                        }
+                        np -= 1;
+                    } else {
+                        st[ip].wt *= ns;
+                        ip += 1;
+                    }
+                } else {
+                    ip += 1;
+                }
+            } while (ip <= np);
+        }
+        if (!Env::kRefOrder) {
+            // transport this photon's charged products before its surviving
+            // photon, so that the stack does not grow with every photon
+            // generation (the reference leaves the survivor among them); the
+            // order of independent particles does not change the expected
+            // dose
+            for (int k = s0 + 1; k <= np; k++)
+                if (st[k].iq == 0) {
+                    Part<double> t = st[s0];
+                    st[s0] = st[k];
+                    st[k] = t;
+                    break;
+                }
+        }
+        if (np < 0 || st[np].iq != 0) return np;
+        eig = st[np].e;
+        irl = st[np].ir;
+        if (eig <= pcut_of(D, irl)) {
+            g.deposit(irl, st[np].wt * eig);
+            return np - 1;
+        }
+        gle = log(eig);
+    }
+}
 
 // shower() (ompmc.c:5454-5465) on a local stack.
 template <typename Env>
@@ -53,16 +184,20 @@ __device__ void shower(const DevData<double> &D, Env &g, Part<double> *st) {
     long steps = 0;
     g.work = 0;
     while (np >= 0) {
-        Part<double> p = st[np];
-        g.top = np;
-        g.nchild = 0;
-        int alive = (p.iq == 0) ? (int)photon_step(D, g, p) : electron_step(D, g, p);
-        if (alive) {
-            st[np] = p;
-            np += g.nchild;
+        if (st[np].iq == 0 && D.nsplit > 1) {
+            np = photon_split(D, g, st, np);
         } else {
-            for (int k = 0; k < g.nchild; k++) st[np + k] = st[np + 1 + k];
-            np += g.nchild - 1;
+            Part<double> p = st[np];
+            g.top = np;
+            g.nchild = 0;
+            int alive = (p.iq == 0) ? (int)photon_step(D, g, p) : electron_step(D, g, p);
+            if (alive) {
+                st[np] = p;
+                np += g.nchild;
+            } else {
+                for (int k = 0; k < g.nchild; k++) st[np + k] = st[np + 1 + k];
+                np += g.nchild - 1;
+            }
         }
         if (++steps > 100000) {
             g.err(ERR_LOOP);
@@ -72,12 +207,14 @@ __device__ void shower(const DevData<double> &D, Env &g, Part<double> *st) {
     }
 }
 
+template <int CAP>
 __global__ void k_plain_beam(DevData<double> D, BeamSrc<double> S, double *endep, uint64_t seed, long hist0, long n,
                              double *src_energy, unsigned *errw) {
     PlainEnv<Philox<double>> g;
-    Part<double> st[PLAIN_STACK];
+    Part<double> st[CAP];
     g.endep = endep;
     g.st = st;
+    g.cap = CAP;
     g.flags = 0;
     double esum = 0;
     for (long h = blockIdx.x * (long)blockDim.x + threadIdx.x; h < n; h += (long)gridDim.x * blockDim.x) {
@@ -91,12 +228,14 @@ __global__ void k_plain_beam(DevData<double> D, BeamSrc<double> S, double *endep
     if (src_energy) atomicAdd(src_energy, esum);
 }
 
+template <int CAP>
 __global__ void k_plain_beamlet(DevData<double> D, BeamletSrc<double> S, int ib, double *endep, uint64_t seed,
                                 long hist0, long n, unsigned *errw) {
     PlainEnv<Philox<double>> g;
-    Part<double> st[PLAIN_STACK];
+    Part<double> st[CAP];
     g.endep = endep;
     g.st = st;
+    g.cap = CAP;
     g.flags = 0;
     for (long h = blockIdx.x * (long)blockDim.x + threadIdx.x; h < n; h += (long)gridDim.x * blockDim.x) {
         g.rng.init(mix64(seed ^ ((uint64_t)ib << 40) ^ (uint64_t)(hist0 + h) * 0x9E3779B97F4A7C15ull),
@@ -157,8 +296,10 @@ struct ScriptRng {
 };
 
 struct ReplayEnv {
+    static constexpr bool kRefOrder = true;
     ScriptRng rng;
     Part<double> *st;
+    int cap;
     int top, nchild;
     unsigned flags;
     int *dep_ir;
@@ -178,7 +319,7 @@ struct ReplayEnv {
     }
     __device__ bool push(const Part<double> &q) {
         int slot = top + 1 + nchild;
-        if (slot >= PLAIN_STACK) {
+        if (slot >= cap) {
             flags |= ERR_STACK;
             return false;
         }
@@ -192,11 +333,13 @@ struct ReplayEnv {
 };
 
 __global__ void k_replay(DevData<double> D, const double *prim, int nhist, const double *rn, const long *rn_off,
-                         int dep_cap, int *dep_ir, double *dep_e, int *ndep, long *nused, unsigned *flags) {
+                         int dep_cap, int *dep_ir, double *dep_e, int *ndep, long *nused, unsigned *flags,
+                         Part<double> *stacks) {
     int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= nhist) return;
     ReplayEnv g;
-    Part<double> st[PLAIN_STACK];
+    Part<double> *st = stacks + (long)h * REPLAY_STACK;
+    g.cap = REPLAY_STACK;
     g.flags = 0;
     g.rng.rn = rn + rn_off[h];
     g.rng.n = rn_off[h + 1] - rn_off[h];
@@ -226,17 +369,39 @@ static int grid_for(omc_engine *e, long n, int block) {
     return (int)(g < 1 ? 1 : g);
 }
 
+// Histories per launch of the plain form: about four seconds of FP64
+// transport, so that a large batch is a sequence of bounded launches.  A
+// history's random stream depends on its index only, so the split does not
+// change the result.
+static const long PLAIN_CHUNK = 1L << 22;
+
 int plain_beam_batch(omc_engine *e, const BeamSrc<double> &S, double *work, uint64_t seed, long hist0, long n,
                      double *src_energy, int block) {
-    k_plain_beam<<<grid_for(e, n, block), block, 0, e->stream>>>(e->d64.d, S, work, seed, hist0, n, src_energy,
-                                                                  e->errword.as<unsigned>());
-    return cuda_check(e, cudaGetLastError(), "k_plain_beam launch");
+    const bool split = e->d64.d.nsplit > 1;
+    for (long c0 = 0; c0 < n; c0 += PLAIN_CHUNK) {
+        long c = std::min(PLAIN_CHUNK, n - c0);
+        if (split)
+            k_plain_beam<SPLIT_STACK><<<grid_for(e, c, block), block, 0, e->stream>>>(
+                e->d64.d, S, work, seed, hist0 + c0, c, src_energy, e->errword.as<unsigned>());
+        else
+            k_plain_beam<PLAIN_STACK><<<grid_for(e, c, block), block, 0, e->stream>>>(
+                e->d64.d, S, work, seed, hist0 + c0, c, src_energy, e->errword.as<unsigned>());
+        int rc = cuda_check(e, cudaGetLastError(), "k_plain_beam launch");
+        if (rc) return rc;
+    }
+    return OMC_OK;
 }
 
 int plain_beamlet_batch(omc_engine *e, const BeamletSrc<double> &S, int ib, double *work, uint64_t seed, long hist0,
                         long n, int block) {
-    k_plain_beamlet<<<grid_for(e, n, block), block, 0, e->stream>>>(e->d64.d, S, ib, work, seed, hist0, n,
-                                                                     e->errword.as<unsigned>());
+    if (e->d64.d.nsplit > 1)
+        k_plain_beamlet<SPLIT_STACK><<<grid_for(e, n, block), block, 0, e->stream>>>(e->d64.d, S, ib, work, seed,
+                                                                                      hist0, n,
+                                                                                      e->errword.as<unsigned>());
+    else
+        k_plain_beamlet<PLAIN_STACK><<<grid_for(e, n, block), block, 0, e->stream>>>(e->d64.d, S, ib, work, seed,
+                                                                                      hist0, n,
+                                                                                      e->errword.as<unsigned>());
     return cuda_check(e, cudaGetLastError(), "k_plain_beamlet launch");
 }
 
@@ -247,10 +412,12 @@ int plain_trace(omc_engine *e, const double *rays_d, int nrays, int cap, double 
     return cuda_check(e, cudaGetLastError(), "k_trace launch");
 }
 
+size_t plain_replay_stack_bytes(int nhist) { return (size_t)nhist * REPLAY_STACK * sizeof(Part<double>); }
+
 int plain_replay(omc_engine *e, const double *prim, int nhist, const double *rn, const long *rn_off, int dep_cap,
-                 int *dep_ir, double *dep_e, int *ndep, long *nused, unsigned *flags) {
+                 int *dep_ir, double *dep_e, int *ndep, long *nused, unsigned *flags, void *stacks) {
     k_replay<<<(nhist + 63) / 64, 64, 0, e->stream>>>(e->d64.d, prim, nhist, rn, rn_off, dep_cap, dep_ir, dep_e, ndep,
-                                                      nused, flags);
+                                                      nused, flags, (Part<double> *)stacks);
     return cuda_check(e, cudaGetLastError(), "k_replay launch");
 }
 

@@ -33,7 +33,7 @@ Errors raise `MexError` with the identifier the MEX entry gives
 mexErrMsgIdAndTxt.  The random numbers are not RANMAR's: `randomSeeds`
 seeds per-bixel Philox streams, so D agrees with the reference within its
 statistical uncertainty rather than bit for bit.  Photon splitting
-(`nSplit` > 1) is not implemented and is rejected.
+(`nSplit` > 1, ompmc.c:1867-2139) is supported up to nSplit = 64.
 """
 from __future__ import annotations
 
@@ -171,8 +171,8 @@ def matrad_dij(cubeRho, cubeMatIx, mcGeo, mcSrc, mcOpt, nargout=1):
     _check_inputs(cubeRho, cubeMatIx, mcGeo, mcSrc)
     cube = _geometry(cubeRho, cubeMatIx, mcGeo)
     nsplit = int(_scalar(_field(mcOpt, "nSplit", required=True)))
-    if nsplit > 1:
-        raise MexError("matRad:omc_matrad:Error", "photon splitting (nSplit > 1) is not implemented")
+    if not 1 <= nsplit <= 64:
+        raise MexError("matRad:omc_matrad:Error", "nSplit must be between 1 and 64")
     ecut = _scalar(_field(mcOpt, "global_ecut", required=True))
     pcut = _scalar(_field(mcOpt, "global_pcut", required=True))
     seeds = np.asarray(_field(mcOpt, "randomSeeds", required=True), dtype=np.float64).ravel()
@@ -186,7 +186,7 @@ def matrad_dij(cubeRho, cubeMatIx, mcGeo, mcSrc, mcOpt, nargout=1):
     device = int(_scalar(_field(mcOpt, "gpuDevice", 0)))
     bl = _source(mcSrc, mcOpt, cube)
     tables = _tables_for(files[0], files[1], files[2], cube.media)
-    eng = Engine(tables, cube, ecut=ecut, pcut=pcut, device=device)
+    eng = Engine(tables, cube, ecut=ecut, pcut=pcut, device=device, nsplit=nsplit)
     try:
         colptr, rows, vals, var, _ = eng.run_beamlets(bl, nhist, nbatch, rel, seed=seed, mode=mode,
                                                       with_variance=nargout >= 2)

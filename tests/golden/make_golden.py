@@ -10,10 +10,12 @@ Fixtures (all seeded; reference RNG seeds 97 33, one thread):
   replay_<case>.npz   primaries, the uniform stream each history consumed
                       (stored exactly as integers rn * 2^24, RANMAR's
                       resolution) and its deposit sequence (region, energy)
+  replaysplit_<case>.npz  the same with photon splitting, nsplit = 20
   dose*_<case>.npz    reference CLI dose and relative uncertainty of the
                       voxels above 5 % of the maximum (8 threads, 50 batches;
                       sources in DOSE: 6 MV and 18 MV photon spectra, 6 MeV
-                      electrons, 3 MeV positrons)
+                      electrons, 3 MeV positrons; dosesplit: 6 MV with
+                      photon splitting, nsplit = 20)
   gamma_<case>.npz    high-statistics reference CLI dose of the voxels above
                       2 % of the maximum for the gamma 2 %/2 mm test (8 threads;
                       water30 1e8, slab64 4e8 histories in 100 batches)
@@ -37,6 +39,7 @@ sys.path.insert(0, str(REPO))
 from ompmc_b200 import assets as A  # noqa: E402
 
 WORK = REPO / "assets" / "golden_work"
+SPLIT = 20      # photon splitting factor of the *split* fixtures (the sample input's value)
 
 CASES = {
     "water30": dict(phantom=lambda: A.water_cube(30, 1.0), collimator=(-5, 5, -5, 5)),
@@ -53,7 +56,7 @@ TABLES = ["ge0", "ge1", "gmfp0", "gmfp1", "gbr10", "gbr11", "gbr20", "gbr21", "c
           "psig_e", "xcc", "blcc", "expeke1", "spin_rej", "ums", "fms", "wms", "ims", "meke"]
 
 
-def case_inp(name, ncase=100000, nbatch=10):
+def case_inp(name, ncase=100000, nbatch=10, nsplit=1):
     """Phantom + spectrum + `.inp` of a case under assets/golden_work."""
     A.require_assets()
     c = CASES[name]
@@ -62,7 +65,8 @@ def case_inp(name, ncase=100000, nbatch=10):
     if not pf.exists():
         A.write_egsphant(pf, ph)
     run = A.default_run(pf, ncase=ncase, nbatch=nbatch, collimator=c["collimator"])
-    base = WORK / f"{name}_{ncase}"
+    run.nsplit = nsplit
+    base = WORK / (f"{name}_{ncase}" if nsplit == 1 else f"{name}_{ncase}_split{nsplit}")
     A.write_inp(base, run)
     return base, ph
 
@@ -125,6 +129,20 @@ def _replay(name, out):
                         dep_e=res["dep_e"], d_off=res["d_off"])
 
 
+def _replaysplit(name, out):
+    """As _replay, with photon splitting (nsplit = SPLIT) and the Russian
+    roulette of photons from electron interactions."""
+    from oracle.ref import Reference
+    base, _ = case_inp(name, nsplit=SPLIT)
+    r = Reference.open(base)
+    nh = 40
+    res = r.run(nh, rn_cap=nh * 60000, dep_cap=nh * 6000)
+    rn_int = np.round(res["rn"] * 16777216.0).astype(np.uint32)
+    assert np.array_equal(rn_int.astype(np.float64) / 16777216.0, res["rn"])
+    np.savez_compressed(out, prim=res["prim"], rn_int=rn_int, rn_off=res["rn_off"], dep_ir=res["dep_ir"],
+                        dep_e=res["dep_e"], d_off=res["d_off"], nsplit=SPLIT)
+
+
 def _tables(name, out):
     from oracle.ref import Reference
     base, _ = case_inp(name)
@@ -143,13 +161,17 @@ DOSE = {
     "dose_ctsmall": ("ctsmall", "6mv", 1.25, 0, 2_000_000),
     "dosee_water30": ("water30", None, 6.0, -1, 1_000_000),
     "dosep_water30": ("water30", None, 3.0, 1, 1_000_000),
+    # photon splitting, nsplit = SPLIT (6th field)
+    "dosesplit_water30": ("water30", "6mv", 1.25, 0, 1_000_000, SPLIT),
+    "dosesplit_slab64": ("slab64", "6mv", 1.25, 0, 1_000_000, SPLIT),
 }
 
 
 def make_dose(fixture, nbatch=50, cores=8):
     """Reference CLI dose of one DOSE entry (voxels above 5 % of the max)."""
     from oracle.ref import run_cli
-    name, spectrum, mono, charge, ncase = DOSE[fixture]
+    name, spectrum, mono, charge, ncase = DOSE[fixture][:5]
+    nsplit = DOSE[fixture][5] if len(DOSE[fixture]) > 5 else 1
     A.require_assets()
     c = CASES[name]
     ph = c["phantom"]()
@@ -158,6 +180,7 @@ def make_dose(fixture, nbatch=50, cores=8):
         A.write_egsphant(pf, ph)
     run = A.default_run(pf, spectrum=spectrum, ncase=ncase, nbatch=nbatch, collimator=c["collimator"],
                         mono_energy=mono, charge=charge)
+    run.nsplit = nsplit
     base = WORK / f"{fixture}_{ncase}"
     A.write_inp(base, run)
     loop_s, _ = run_cli(base, f"golden_{fixture}", cores=cores)
@@ -166,7 +189,7 @@ def make_dose(fixture, nbatch=50, cores=8):
     np.savez_compressed(HERE / f"{fixture}.npz", idx=keep.astype(np.int32), dose=dose.ravel()[keep],
                         unc=unc.ravel()[keep].astype(np.float32), shape=np.array(dose.shape), dmax=dose.max(),
                         ncase=ncase, nbatch=nbatch, loop_seconds=loop_s, cores=cores,
-                        spectrum=str(spectrum or ""), mono_energy=mono, charge=charge)
+                        spectrum=str(spectrum or ""), mono_energy=mono, charge=charge, nsplit=nsplit)
 
 
 GAMMA_HIST = {"water30": 100_000_000, "slab64": 400_000_000}
@@ -221,7 +244,7 @@ def main():
     build()
     A.require_assets()
     WORK.mkdir(parents=True, exist_ok=True)
-    jobs = [("rays", n) for n in CASES] + [("replay", n) for n in CASES]
+    jobs = [("rays", n) for n in CASES] + [("replay", n) for n in CASES] + [("replaysplit", n) for n in CASES]
     for what, name in jobs:
         fn = f"{what}_{name}"
         if a.only and a.only not in fn:

@@ -6,16 +6,28 @@ creation, and FP32 directions are renormalised inside the physics, so where
 a cycle cuts a particle's transport is invisible in its trajectory.  The
 dose of a run with the smallest fixed budgets (one photon interaction, one
 electron tstep-loop iteration per event) equals the dose with the adaptive
-drain-tail budgets and with large fixed ones, up to the summation order of
-the FP64 tally atomics (rtol 1e-9 per voxel)."""
+drain-tail budgets, with large fixed ones and with the electron queues
+regrouped by energy, smaller blocks and fewer particles in flight, up to the
+summation order of the FP64 tally atomics (rtol 1e-9 per voxel)."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
+CONFIGS = {
+    "nsplit1": [dict(electron_tsteps=1, tail_boost=1, electron_split=0.0), dict(),
+                dict(electron_tsteps=7, tail_boost=64), dict(electron_split=1.0, block=128, inflight=1 << 18)],
+    # photon splitting: a split photon's state (sub-photon, survivor,
+    # stratification offset) is carried from event to event
+    "nsplit5": [dict(nsplit=5, electron_tsteps=1, tail_boost=1, electron_split=0.0), dict(nsplit=5),
+                dict(nsplit=5, block=128, inflight=1 << 18)],
+}
+
+
+@pytest.mark.parametrize("split", ["nsplit1", "nsplit5"])
 @pytest.mark.parametrize("case", ["slab64", "ctsmall"])
-def test_dose_independent_of_event_budgets(case, assets_root):
+def test_dose_independent_of_event_budgets(case, split, assets_root):
     from ompmc_b200.engine import EVENT_FP32, Engine, Tables, load_spectrum
     from tests.conftest import CASES, case_phantom
     ph = case_phantom(case)
@@ -23,9 +35,9 @@ def test_dose_independent_of_event_budgets(case, assets_root):
     spec = load_spectrum(assets_root / "spectra" / "6mv.spectrum")
     coll = CASES[case]["collimator"]
     doses = []
-    for kw in (dict(electron_tsteps=1, tail_boost=1), dict(), dict(electron_tsteps=7, tail_boost=64)):
+    for kw in CONFIGS[split]:
         eng = Engine(t, ph, **kw)
-        d, u, st = eng.run_beam(200000, 10, seed=4242, mode=EVENT_FP32, spectrum=spec, collimator=coll)
+        d, u, st = eng.run_beam(200000 if split == "nsplit1" else 50000, 10, seed=4242, mode=EVENT_FP32, spectrum=spec, collimator=coll)
         assert st["flags"] == 0
         doses.append(d)
         eng.close()

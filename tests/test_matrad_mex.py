@@ -40,7 +40,7 @@ def mex_inputs(assets_root, golden, nhist=None):
     (lambda a: a.__setitem__(3, None), "MATLAB:phonebook:inputNotStruct"),
     (lambda a: a[2].pop("material"), "matRad:omc_matrad:Error"),
     (lambda a: a[4].pop("global_ecut"), "matRad:omc_matrad:Error"),
-    (lambda a: a[4].__setitem__("nSplit", 4), "matRad:omc_matrad:Error"),
+    (lambda a: a[4].__setitem__("nSplit", 65), "matRad:omc_matrad:Error"),
     (lambda a: a[4].__setitem__("spectrumFile", "/nonexistent/x.spectrum"), "matRad:omc_matrad:Error"),
 ], ids=["rho_not_double", "rho_not_3d", "matix_not_int32", "geo_not_struct", "src_not_struct",
         "no_materials", "missing_ecut", "nsplit", "no_spectrum"])

@@ -16,17 +16,22 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def replay_case(case, golden, engine_for):
-    g = golden(f"replay_{case}")
+def replay_case(case, golden, engine_for, fixture="replay"):
+    g = golden(f"{fixture}_{case}")
     rn = g["rn_int"].astype(np.float64) / 16777216.0
-    eng = engine_for(case)
-    dir_, de, nd, nu, fl = eng.replay(g["prim"], rn, g["rn_off"], dep_cap=4096)
+    ns = int(g.get("nsplit", 1))
+    eng = engine_for(case, nsplit=ns) if ns > 1 else engine_for(case)
+    dir_, de, nd, nu, fl = eng.replay(g["prim"], rn, g["rn_off"], dep_cap=8192)
     return g, dir_, de, nd, nu, fl
 
 
 @pytest.mark.parametrize("case", ["water30", "slab64", "ctsmall"])
-def test_replay_matches_reference(case, golden, engine_for):
-    g, dir_, de, nd, nu, fl = replay_case(case, golden, engine_for)
+@pytest.mark.parametrize("fixture", ["replay", "replaysplit"])
+def test_replay_matches_reference(fixture, case, golden, engine_for):
+    """replaysplit: photon splitting with nsplit = 20 (each photon
+    interaction sampled 20 times at weight 1/20, Russian roulette of photons
+    made by electrons), the sample input's setting."""
+    g, dir_, de, nd, nu, fl = replay_case(case, golden, engine_for, fixture)
     nh = len(g["prim"])
     rn_len = np.diff(g["rn_off"])
     d_len = np.diff(g["d_off"])
