@@ -393,7 +393,7 @@ def main():
         prof_eng = Engine(tables, ph, ecut=0.7, pcut=0.01, device=local, profile=True)
         if tuned:
             prof_eng.event_params(**{k: tuned[k] for k in ("electron_tsteps", "tail_boost", "inflight", "block",
-                                                           "electron_split")})
+                                                           "electron_split", "electron_chsteps")})
         prof_eng.run_beam(nstep, NBATCH, seed=777, mode=EVENT_FP32, spectrum=spec, collimator=COLLIMATOR)
         prof = prof_eng.profile_last()
         prof_eng.close()
@@ -414,7 +414,9 @@ def main():
             "state_bytes_per_launch": 104 * per_launch_events,
             "achieved_with_state": (alg_bytes + 104 * ek["particles"]) / ek["seconds"] / 1e9,
             "avg_launch_ms": 1000 * ek["seconds"] / max(1, ek["launches"]),
-            "kernel_share": {k: v["seconds"] for k, v in prof.items()},
+            "kernel_seconds": {k: v["seconds"] for k, v in prof.items()},
+            "kernel_share": {k: v["seconds"] / max(1e-12, sum(x["seconds"] for x in prof.values()))
+                             for k, v in prof.items()},
         }
         hist = nstep
         per_hist = {k: ek[k] / hist + pk[k] / hist for k in ("particles", "steps", "cross", "dep", "atom")}
@@ -437,6 +439,19 @@ def main():
             _, _, pst = step(1000, m=PLAIN_FP64, n=pn)
             plain = pn / pst["seconds"]
             extras["plain_fp64"] = {"value": plain, "unit": "histories/s", "speedup_event_vs_plain": value / plain}
+            # photon splitting (nsplit = 20, the reference's sample input):
+            # fewer histories/s, lower variance per history; compared by the
+            # time to 1 % mean uncertainty in voxels above 50 % of the maximum
+            sn = max(nstep // 4, 100000)
+            se = Engine(tables, ph, ecut=0.7, pcut=0.01, device=local, nsplit=20)
+            step(998, e=se, n=sn)
+            sd, su, sst = step(997, e=se, n=sn)
+            se.close()
+            su1 = mean_unc_above_half(sd, su)
+            srate = sn / sst["seconds"]
+            extras["nsplit20"] = {"value": srate, "unit": "histories/s", "histories": sn,
+                                  "mean_rel_unc_gt50pct_dmax": su1,
+                                  "seconds_to_1pct": sn * (su1 / 0.01) ** 2 / srate}
             # CPU reference on this host's cores (bounded sample)
             from oracle import ref
             if ref.available():
