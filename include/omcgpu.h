@@ -87,7 +87,7 @@ typedef struct {
     int profile;          /* 1: event form launches cycles one by one and times
                              every kernel (see omc_profile_last) */
     int electron_tsteps;  /* event form: tstep-loop iterations an electron runs
-                             per launch before it is re-queued (0 = default) */
+                             per launch before it is re-queued (0 = default 1) */
     int64_t inflight;     /* event form: particles kept in flight (0 = default) */
     int tail_boost;       /* event form: largest factor by which event budgets
                              grow as the queues drain (0 = default 32, 1 = fixed
@@ -96,6 +96,12 @@ typedef struct {
                              (MeV) are queued apart from the others so that
                              warps see particles of one kind (0 = one group,
                              default 0.3); results do not depend on it */
+    int electron_chsteps; /* event form: condensed-history steps after which an
+                             electron's distance to its next discrete
+                             interaction is drawn afresh (memoryless, so the
+                             sampled physics is the same; default 2; 0 = the
+                             reference's restart after every step, which
+                             also costs a zero-length step each time) */
 } omc_options;
 
 void omc_options_default(omc_options *o);
@@ -105,11 +111,13 @@ typedef struct omc_engine omc_engine;
 int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_options *o, omc_engine **out);
 int omc_engine_destroy(omc_engine *e);
 /* Event-form tuning parameters of a live engine (the options of the same
- * names; a value <= 0 keeps the current one, for electron_split < 0).  Results do not depend on
- * them (up to the summation order of the FP64 tallies); the autotuner
- * (ompmc_b200/autotune.py) sweeps them. */
+ * names; a value <= 0 keeps the current one, for electron_split and
+ * electron_chsteps a value < 0).  Dose does not depend on the first five
+ * (up to the summation order of the FP64 tallies) and its distribution
+ * not on electron_chsteps; the autotuner (ompmc_b200/autotune.py) sweeps
+ * them. */
 int omc_event_params(omc_engine *e, int electron_tsteps, int tail_boost, int64_t inflight, int block,
-                     double electron_split);
+                     double electron_split, int electron_chsteps);
 const char *omc_engine_last_error(const omc_engine *e);
 
 /* Per-kernel profile of the last event-form omc_run_beam made with

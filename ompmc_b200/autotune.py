@@ -12,7 +12,9 @@ for speed per phantom, source and GPU:
 * block           — threads per block of the transport kernels (whole warps,
                     at most 256, their launch bound);
 * electron_split  — regroup energy: electrons above it (kinetic, MeV) are
-                    queued apart from the others (0 = one group).
+                    queued apart from the others (0 = one group);
+* electron_chsteps — condensed-history steps between re-draws of an
+                    electron's distance to its next discrete interaction.
 
 `tune_beam` runs short dose runs of the given beam on a live engine and
 searches the space coordinate by coordinate (each parameter swept with the
@@ -32,8 +34,10 @@ SPACE = {
     "inflight": [1 << 18, 1 << 19, 1 << 20, 1 << 21],
     "block": [64, 128, 256],
     "electron_split": [0.0, 0.2, 0.3, 0.5, 1.0],
+    "electron_chsteps": [1, 2, 4, 8],
 }
-DEFAULT = {"electron_tsteps": 2, "tail_boost": 32, "inflight": 1 << 20, "block": 256, "electron_split": 0.3}
+DEFAULT = {"electron_tsteps": 1, "tail_boost": 32, "inflight": 1 << 20, "block": 256, "electron_split": 0.3,
+           "electron_chsteps": 2}
 
 
 def _rate(eng, cfg, nhist, run_kw, repeats):

@@ -94,6 +94,9 @@ struct DevData {
     R b2spin_min, dbeta2i, espml, dleneri, dqq1i, dllambi, dqmsi;
     int ref_compat;                  // reproduce reference quirks (default 1)
     int nsplit;                      // photon splitting factor (1 = off)
+    int chsteps;                     // electrons: condensed-history steps after which the
+                                     // distance to the next discrete interaction is re-drawn
+                                     // (0 = the reference's restart after every step)
 };
 
 // Beam source of the dosxyz ucode (omc_dosxyz.c:337-632, :964-1068).

@@ -195,6 +195,10 @@ static int build_devset(omc_engine *e, DevSet<R> &S) {
     S.d = L.d;
     DevData<R> &d = S.d;
     d.nsplit = e->opt.nsplit > 1 ? e->opt.nsplit : 1;
+    // the plain FP64 form keeps the reference's per-step restart (its
+    // trajectories replay the reference's); the event form re-draws after
+    // electron_chsteps steps
+    d.chsteps = sizeof(R) == 4 ? std::max(0, e->opt.electron_chsteps) : 0;
     d.xb = S.xb.template as<R>(); d.yb = S.yb.template as<R>(); d.zb = S.zb.template as<R>();
     d.med = S.med.template as<int8_t>(); d.rhof = S.rhof.template as<R>();
     d.ms = S.ms.template as<MedS<R>>(); d.ph = S.ph.template as<PhBin<R>>(); d.pmax = S.pmax.template as<PL<R>>();
@@ -476,6 +480,7 @@ void omc_options_default(omc_options *o) {
     o->block = 0;
     o->nsplit = 1;
     o->electron_split = 0.3;
+    o->electron_chsteps = 2;
 }
 
 int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_options *o, omc_engine **out) {
@@ -550,9 +555,13 @@ int omc_engine_destroy(omc_engine *e) {
 const char *omc_engine_last_error(const omc_engine *e) { return e ? e->err.c_str() : omc_last_error(); }
 
 int omc_event_params(omc_engine *e, int electron_tsteps, int tail_boost, int64_t inflight, int block,
-                     double electron_split) {
+                     double electron_split, int electron_chsteps) {
     if (!e) return global_err(OMC_E_ARG, "omc_event_params: null engine");
     cudaSetDevice(e->device);
+    if (electron_chsteps >= 0) {
+        e->opt.electron_chsteps = electron_chsteps;
+        e->d32.d.chsteps = electron_chsteps;
+    }
     return event_set_params(e, electron_tsteps, tail_boost, (long long)inflight, block, electron_split);
 }
 

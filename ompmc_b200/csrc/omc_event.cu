@@ -513,8 +513,9 @@ int event_prepare(omc_engine *e) {
     S.block = e->opt.block > 0 ? std::min(EV_MAX_BLOCK, (e->opt.block + 31) / 32 * 32) : 256;
     S.grid = e->sm_count * std::max(1, 2048 / S.block);
     size_grids(e, S);
-    // 2 measured best on the slab workload while the queues are full
-    S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 2;
+    // 1 measured best on the slab workload while the queues are full (with
+    // the default electron_chsteps = 2: at most two CH steps per event)
+    S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 1;
     S.boost = e->opt.tail_boost > 0 ? e->opt.tail_boost : 32;
     S.inflight = e->opt.inflight > 0 ? e->opt.inflight : (1LL << 20);
     S.esplit = e->opt.electron_split > 0 ? e->opt.electron_split + D_RM : 0.0;
@@ -551,7 +552,7 @@ int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, i
     }
     if (e->ev && e->ev->ready) {
         EventState &S = *e->ev;
-        S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 2;
+        S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 1;
         S.boost = e->opt.tail_boost > 0 ? e->opt.tail_boost : 32;
         S.inflight = e->opt.inflight > 0 ? e->opt.inflight : (1LL << 20);
         S.esplit = e->opt.electron_split > 0 ? e->opt.electron_split + D_RM : 0.0;

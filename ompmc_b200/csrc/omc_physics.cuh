@@ -1297,13 +1297,30 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
                 sig0 = M.sige[qel];
             }
         }
+        int nch = 0;            // condensed-history steps of this tstep iteration
+        bool redraw = false;
         do {  // ustep loop
+            if (D.chsteps > 0) {
+                // after chsteps steps the remaining distance to the next
+                // discrete interaction is drawn afresh at the top of the
+                // tstep loop: the number of mean free paths to it is
+                // exponential, hence memoryless, so the re-draw samples the
+                // same distribution (the reference restarts after every
+                // step, below; EGSnrc never)
+                if (nch == D.chsteps) {
+                    redraw = true;
+                    break;
+                }
+                nch++;
+            }
             if (++guard > 20000 || !g.tick()) { g.err(ERR_LOOP); return E_DEAD; }
-            // quirk: the reference declares total_tstep inside this loop
-            // (ompmc.c:4799), so every step after the first of a tstep cycle
-            // sees tstep = 0, takes a zero-length single-scattering step
-            // (one draw) and restarts the cycle with a new demfp.
-            if (D.ref_compat) total_tstep = R(0);
+            if (D.chsteps <= 0 && D.ref_compat) {
+                // quirk: the reference declares total_tstep inside this loop
+                // (ompmc.c:4799), so every step after the first of a tstep
+                // cycle sees tstep = 0, takes a zero-length single-scattering
+                // step (one draw) and restarts the cycle with a new demfp.
+                total_tstep = R(0);
+            }
             bool call_howfar, do_single = false, called_msdist = false;
             R tstep, tustep, de = 0, tvstep = 0, range = 0;
             R xf = 0, yf = 0, zf = 0, uf = 0, vf = 0, wf = 0;
@@ -1495,7 +1512,7 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
             total_tstep -= tvstep * rhof;
             if (total_tstep < R(1.0E-9)) demfp = R(0);
         } while (demfp >= R(1.0E-5));
-        if ((imed != medold) || (ustep == R(0)) || (imed == -1)) continue;
+        if (redraw || (imed != medold) || (ustep == R(0)) || (imed == -1)) continue;
         const ElBin<R> &B = ebin(D, imed, qel, lelke);
         R sigf = pwl(B.sig, elke);
         R dedx0 = pwl(B.dedx, elke);

@@ -50,7 +50,8 @@ class _Options(C.Structure):
     _fields_ = [("ecut", C.c_double), ("pcut", C.c_double), ("device", C.c_int),
                 ("ref_compat", C.c_int), ("queue_capacity", C.c_int64), ("block", C.c_int),
                 ("nsplit", C.c_int), ("profile", C.c_int), ("electron_tsteps", C.c_int),
-                ("inflight", C.c_int64), ("tail_boost", C.c_int), ("electron_split", C.c_double)]
+                ("inflight", C.c_int64), ("tail_boost", C.c_int), ("electron_split", C.c_double),
+                ("electron_chsteps", C.c_int)]
 
 
 class _Energy(C.Structure):
@@ -101,7 +102,7 @@ def lib():
         "omc_dosxyz_run": ([C.c_char_p, C.c_char_p, C.c_int, C.c_int], C.c_int),
         "omc_profile_last": ([C.c_void_p, _dp, C.c_int], C.c_int),
         "omc_profile_trace": ([C.c_void_p, _dp, C.c_int], C.c_int),
-        "omc_event_params": ([C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int, C.c_double], C.c_int),
+        "omc_event_params": ([C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int, C.c_double, C.c_int], C.c_int),
         "omc_run_beam_noalloc": ([C.c_void_p, C.POINTER(_Beam), C.c_int64, C.c_int, C.c_uint64, _dp, _dp, _dp],
                                  C.c_int),
         "omc_server_create": ([C.c_void_p, C.c_int64, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)], C.c_int),
@@ -196,7 +197,7 @@ class Engine:
 
     def __init__(self, tables: Tables, phantom, ecut=0.7, pcut=0.01, device=0, ref_compat=True,
                  queue_capacity=0, block=0, profile=False, electron_tsteps=0, inflight=0, tail_boost=0,
-                 electron_split=None, nsplit=1):
+                 electron_split=None, nsplit=1, electron_chsteps=None):
         L = lib()
         self.tables = tables
         self.phantom = phantom
@@ -222,6 +223,8 @@ class Engine:
         o.tail_boost = tail_boost
         if electron_split is not None:
             o.electron_split = electron_split
+        if electron_chsteps is not None:
+            o.electron_chsteps = int(electron_chsteps)
         h = C.c_void_p()
         _check(L.omc_engine_create(tables.h, C.byref(P), C.byref(o), C.byref(h)))
         self.h = h
@@ -342,11 +345,12 @@ class Engine:
         return {names[k]: dict(zip(keys, out[k * 7:(k + 1) * 7])) for k in range(4)}
 
     # ------------------------------------------------ validation hooks
-    def event_params(self, electron_tsteps=0, tail_boost=0, inflight=0, block=0, electron_split=-1.0):
-        """Event-form tuning parameters (0, or -1 for electron_split, keeps
-        the current value)."""
+    def event_params(self, electron_tsteps=0, tail_boost=0, inflight=0, block=0, electron_split=-1.0,
+                     electron_chsteps=-1):
+        """Event-form tuning parameters (0, or -1 for electron_split and
+        electron_chsteps, keeps the current value)."""
         _check(lib().omc_event_params(self.h, int(electron_tsteps), int(tail_boost), int(inflight), int(block),
-                                      float(electron_split)), self.h)
+                                      float(electron_split), int(electron_chsteps)), self.h)
 
     def profile_trace(self):
         """Per-cycle trace of the last profiled event-form run: array of rows
