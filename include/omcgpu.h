@@ -183,7 +183,10 @@ typedef struct {
  * voxels with rho < 0.044 zeroed).  dose/unc: nvox doubles (may be NULL).
  * stats (may be NULL) receives [0] histories run, [1] device seconds of the
  * transport, [2] kernel launches, [3] deposited energy (MeV), [4] source
- * energy (MeV), [5] error flags. */
+ * energy (MeV), [5] error flags.  The engine keeps the run's device
+ * buffers (tallies, sums, outputs; event form: nbatch*nvox batch tallies)
+ * between calls, so repeated runs allocate nothing; they are released
+ * with the engine. */
 int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, uint64_t seed, int mode,
                  double *dose, double *unc, double *stats);
 

@@ -601,9 +601,10 @@ int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, ui
     long nper = (long)(ncase / nbatch);
     long nv = e->ph.nvox();
     int rc;
-    DBuf sum, sum2, out_d, unc_d, cdf, acc;
-    if ((rc = sum.alloc(nv * 8)) || (rc = sum2.alloc(nv * 8)) || (rc = out_d.alloc(nv * 8)) ||
-        (rc = unc_d.alloc(nv * 8)) || (rc = acc.alloc(4 * 8)))
+    DBuf &sum = e->run_sum, &sum2 = e->run_sum2, &out_d = e->run_out, &unc_d = e->run_unc, &cdf = e->run_cdf,
+         &acc = e->run_acc;
+    if ((rc = sum.reserve(nv * 8)) || (rc = sum2.reserve(nv * 8)) || (rc = out_d.reserve(nv * 8)) ||
+        (rc = unc_d.reserve(nv * 8)) || (rc = acc.reserve(4 * 8)))
         return set_err(e, rc, "device allocation for tallies failed");
     cudaMemsetAsync(sum.p, 0, nv * 8, e->stream);
     cudaMemsetAsync(sum2.p, 0, nv * 8, e->stream);
@@ -616,13 +617,14 @@ int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, ui
         if (ncdf > 0) {
             c.assign(b->energy.cdf1, b->energy.cdf1 + ncdf);
             c.insert(c.end(), b->energy.cdf2, b->energy.cdf2 + ncdf);
-            if ((rc = upload(e, cdf, c))) return rc;
+            if ((rc = cdf.reserve(c.size() * 8))) return set_err(e, rc, "device allocation failed");
+            cudaMemcpyAsync(cdf.p, c.data(), c.size() * 8, cudaMemcpyHostToDevice, e->stream);
         }
         BeamSrc<double> S = beam_setup<double>(e, b);
         S.cdf1 = ncdf > 0 ? cdf.as<double>() : nullptr;
         S.cdf2 = ncdf > 0 ? cdf.as<double>() + ncdf : nullptr;
-        DBuf work;
-        if ((rc = work.alloc(nv * 8))) return set_err(e, rc, "device allocation for tallies failed");
+        DBuf &work = e->run_work;
+        if ((rc = work.reserve(nv * 8))) return set_err(e, rc, "device allocation for tallies failed");
         cudaMemsetAsync(work.p, 0, nv * 8, e->stream);
         int block = e->opt.block > 0 ? e->opt.block : 128;
         cudaEvent_t t0, t1;

@@ -26,6 +26,8 @@ struct DBuf {
         n = 0;
     }
     int alloc(size_t bytes);
+    // keep the buffer if it holds `bytes` already, else reallocate
+    int reserve(size_t bytes) { return (p && n >= bytes) ? 0 : alloc(bytes); }
     template <typename T>
     T *as() const { return (T *)p; }
 };
@@ -84,6 +86,9 @@ struct omc_engine {
     std::string err;
     std::vector<double> mass;  // voxel mass (g), host copy
     omc::DBuf mass_d;
+    // device buffers of omc_run_beam, kept between calls and grown on
+    // demand so that a run allocates nothing once the engine is warm
+    omc::DBuf run_sum, run_sum2, run_out, run_unc, run_acc, run_cdf, run_work, run_tal, run_cdf32;
 };
 
 namespace omc {

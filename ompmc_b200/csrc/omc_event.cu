@@ -380,8 +380,10 @@ __global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_split_step(DevData<floa
 
 // Electron/positron events of the queued charged particles: at most the
 // cycle's budget of tstep-loop iterations each, then the particle is
-// re-queued.
-__global__ void __launch_bounds__(EV_MAX_BLOCK) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
+// re-queued.  Four resident blocks of 256 threads per SM (64 registers,
+// a few spills) measured faster than three (80) or two (114): the step is
+// latency bound and more warps hide more of it.
+__global__ void __launch_bounds__(EV_MAX_BLOCK, 4) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
                                                        double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
                                                        int *live, int nbmax) {
     transport_events<EV_ELECTRON>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax);
@@ -654,15 +656,15 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
     if (rc) return rc;
     EventState &S = *e->ev;
     long nvox = e->ph.nvox();
-    DBuf tal, cdf;
-    if ((rc = tal.alloc((size_t)nbatch * nvox * 8))) return set_err(e, rc, "batch tallies allocation failed");
+    DBuf &tal = e->run_tal, &cdf = e->run_cdf32;
+    if ((rc = tal.reserve((size_t)nbatch * nvox * 8))) return set_err(e, rc, "batch tallies allocation failed");
     cudaMemsetAsync(tal.p, 0, (size_t)nbatch * nvox * 8, e->stream);
     int ncdf = b->energy.n;
     BeamSrc<float> src = beam_setup<float>(e, b);
     if (ncdf > 0) {
         std::vector<float> c(b->energy.cdf1, b->energy.cdf1 + ncdf);
         c.insert(c.end(), b->energy.cdf2, b->energy.cdf2 + ncdf);
-        if ((rc = cdf.alloc(c.size() * 4))) return set_err(e, rc, "alloc");
+        if ((rc = cdf.reserve(c.size() * 4))) return set_err(e, rc, "alloc");
         cudaMemcpyAsync(cdf.p, c.data(), c.size() * 4, cudaMemcpyHostToDevice, e->stream);
         src.cdf1 = cdf.as<float>();
         src.cdf2 = cdf.as<float>() + ncdf;
