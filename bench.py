@@ -338,8 +338,13 @@ def main():
     nstep = args.hist_per_step
     seed0 = rank_seed(rank)
 
+    # results land in pinned host buffers (the e2e copy is a DMA from the device)
+    nv = int(np.prod(eng.shape))
+    pinned = tuple(torch.empty(nv, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2))
+
     def step(i, e=eng, m=mode, n=nstep):
-        return e.run_beam(n, NBATCH, seed=seed0 + i, mode=m, spectrum=spec, collimator=COLLIMATOR)
+        return e.run_beam(n, NBATCH, seed=seed0 + i, mode=m, spectrum=spec, collimator=COLLIMATOR,
+                          out=pinned if e is eng else None)
 
     if args.cycle_trace:
         # same seed as the first warm-up step: the queue sizes per cycle are

@@ -253,17 +253,24 @@ class Engine:
         return e
 
     def run_beam(self, ncase, nbatch=10, seed=1, mode=EVENT_FP32, spectrum=None, mono_energy=1.25, charge=0,
-                 ssd=100.0, collimator=(-5.0, 5.0, -5.0, 5.0)):
+                 ssd=100.0, collimator=(-5.0, 5.0, -5.0, 5.0), out=None):
         """Dose (Gy per history) and relative uncertainty arrays [nz,ny,nx]
-        plus a stats dict; the dosxyz beam source (omc_dosxyz.c:964-1068)."""
+        plus a stats dict; the dosxyz beam source (omc_dosxyz.c:964-1068).
+        `out`: optional (dose, unc) float64 arrays of nvox elements to write
+        into (e.g. pinned host memory)."""
         keep = []
         b = _Beam()
         b.energy = self._energy(spectrum, mono_energy, charge, keep)
         b.ssd = ssd
         b.xinl, b.xinu, b.yinl, b.yinu = collimator
         n = int(np.prod(self.shape))
-        dose = np.zeros(n)
-        unc = np.zeros(n)
+        if out is not None:
+            dose, unc = out
+            assert dose.dtype == np.float64 and unc.dtype == np.float64 and dose.size == n and unc.size == n
+            assert dose.flags.c_contiguous and unc.flags.c_contiguous
+        else:
+            dose = np.zeros(n)
+            unc = np.zeros(n)
         st = np.zeros(6)
         _check(lib().omc_run_beam(self.h, C.byref(b), int(ncase), int(nbatch), int(seed) & (2**64 - 1), mode,
                                   _p(dose, _dp), _p(unc, _dp), _p(st, _dp)), self.h)

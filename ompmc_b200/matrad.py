@@ -167,7 +167,7 @@ def matrad_dij(cubeRho, cubeMatIx, mcGeo, mcSrc, mcOpt, nargout=1):
     scipy.sparse.csc_matrix of shape (nx*ny*nz, nBixels)."""
     import scipy.sparse as sp
     if nargout > 2:
-        raise MexError("matRad:omc_matrad:invalidNumOutputs", "Too many output arguments")
+        raise MexError("matRad:matRad_ompInterface:invalidNumOutputs", "Too many output arguments.")
     _check_inputs(cubeRho, cubeMatIx, mcGeo, mcSrc)
     cube = _geometry(cubeRho, cubeMatIx, mcGeo)
     nsplit = int(_scalar(_field(mcOpt, "nSplit", required=True)))

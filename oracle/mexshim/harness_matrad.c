@@ -161,6 +161,7 @@ void mxSetIr(mxArray *a, mwIndex *p) { a->ir = p; }
 void mxSetNzmax(mxArray *a, mwSize n) { a->nzmax = n; }
 void *mxRealloc(void *p, size_t n) { return realloc(p, n ? n : 1); }
 void *mxCalloc(size_t n, size_t sz) { return calloc(n ? n : 1, sz ? sz : 1); }
+void mxFree(void *p) { free(p); }
 
 int mexPrintf(const char *fmt, ...) {
     if (g_quiet) return 0;

@@ -61,6 +61,7 @@ void mxSetIr(mxArray *a, mwIndex *p);
 void mxSetNzmax(mxArray *a, mwSize n);
 void *mxRealloc(void *p, size_t n);
 void *mxCalloc(size_t n, size_t sz);
+void mxFree(void *p);
 mxArray *mxCreateDoubleScalar(double v);
 mxArray *mxCreateString(const char *s);
 void mxDestroyArray(mxArray *a);

@@ -173,23 +173,27 @@ class Reference:
 
 
 MATRAD_LIB = REF_DIR / "libompmc_matrad_ref.so"
-_matrad = None
+
+
+_mex_libs = {}
 
 
 def matrad_dij(phantom, beamlets, nhist, nbatch=10, seeds=(97, 33), ecut=0.7, pcut=0.01, rel_threshold=1e-4,
-               spectrum_file="", assets_root=None, gaussian=False, gauss_width=0.2123, cap=None):
+               spectrum_file="", assets_root=None, gaussian=False, gauss_width=0.2123, cap=None, lib=None):
     """One call of the unmodified matRad MEX entry (omc_matrad.c:1417) through
     the mex.h shim.  `beamlets` is the dict of ompmc_b200.engine.bixel_grid
-    (0-based ibeam).  Returns (colptr, rows, vals, var) of D and V."""
-    global _matrad
+    (0-based ibeam).  Returns (colptr, rows, vals, var) of D and V.  `lib`:
+    another build of the shim harness linked with a different mexFunction
+    (the tests use it to drive this project's MEX entry the same way)."""
     from ompmc_b200 import assets as A
     root = Path(assets_root) if assets_root else A.require_assets()
-    if _matrad is None:
-        L = C.CDLL(str(MATRAD_LIB))
+    path = str(lib or MATRAD_LIB)
+    if path not in _mex_libs:
+        L = C.CDLL(path)
         L.hm_dij.restype = C.c_long
         L.hm_last_error.restype = C.c_char_p
-        _matrad = L
-    L = _matrad
+        _mex_libs[path] = L
+    L = _mex_libs[path]
     nx, ny, nz = phantom.shape
     rho = np.ascontiguousarray(phantom.rho, dtype=np.float64).ravel()
     mat = np.ascontiguousarray(phantom.med, dtype=np.int32).ravel()

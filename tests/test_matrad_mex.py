@@ -82,3 +82,65 @@ def test_mirror_matches_matrad_reference(transport, assets_root, golden):
     assert len(z) > 250
     assert np.mean(np.abs(z) < 3) >= 0.99, np.mean(np.abs(z) < 3)
     assert abs(z.mean()) < 0.25
+
+
+# ------------------------------------------------ the C MEX entry
+# ompmc_b200/mex/omc_matrad_gpu.c is what a MATLAB user compiles with `mex`;
+# here it is compiled against the mex.h stand-in of the oracle and driven by
+# the same harness that runs the unmodified reference entry.
+
+def build_mex_shim(tmp_dir):
+    """Shared library of the shim harness linked with omc_matrad_gpu.c."""
+    import subprocess
+    from tests.conftest import REPO
+    shim = REPO / "oracle" / "mexshim"
+    out = tmp_dir / "libomc_matrad_gpu_shim.so"
+    steps = [["gcc", "-O2", "-fPIC", "-std=c99", "-Wall", "-Wextra", "-Werror", f"-I{shim}", f"-I{REPO / 'include'}",
+              "-c", str(REPO / "ompmc_b200" / "mex" / "omc_matrad_gpu.c"), "-o", str(tmp_dir / "mex.o")],
+             ["gcc", "-O2", "-fPIC", "-w", f"-I{shim}", "-c", str(shim / "harness_matrad.c"),
+              "-o", str(tmp_dir / "shim.o")],
+             ["gcc", "-shared", str(tmp_dir / "mex.o"), str(tmp_dir / "shim.o"), f"-L{REPO / 'ompmc_b200'}",
+              "-lomcgpu", f"-Wl,-rpath,{REPO / 'ompmc_b200'}", "-lm", "-o", str(out)]]
+    for cmd in steps:
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        assert p.returncode == 0, p.stderr[-2000:]
+    return out
+
+
+def test_mex_entry_builds_against_mex_api(tmp_path):
+    """The MEX source compiles warning-free against the mx/mex API subset
+    and exports mexFunction (no device needed)."""
+    import ctypes
+    lib = ctypes.CDLL(str(build_mex_shim(tmp_path)))
+    assert hasattr(lib, "mexFunction") and hasattr(lib, "hm_dij")
+
+
+@pytest.mark.gpu
+def test_mex_entry_matches_matrad_reference(tmp_path, assets_root, golden):
+    """D and V of the C MEX entry (event form, the default) against the
+    unmodified reference entry's fixture, as for the Python mirror."""
+    from oracle.ref import matrad_dij as shim_dij
+    from tests.conftest import case_phantom
+    g = golden("dij_ctsmall")
+    lib = build_mex_shim(tmp_path)
+    ph = case_phantom("ctsmall")
+    bl = dict(src=g["src"], corner=g["corner"], side1=g["side1"], side2=g["side2"], ibeam=g["ibeam"])
+    colptr, rows, vals, var = shim_dij(ph, bl, int(g["nhist"]), int(g["nbatch"]), seeds=(97, 33),
+                                       rel_threshold=float(g["rel"]),
+                                       spectrum_file=str(assets_root / "spectra" / "6mv.spectrum"), lib=lib)
+    nvox = int(np.prod(ph.shape))
+    zs = []
+    for i in range(len(g["corner"])):
+        rr = g["rows"][g["colptr"][i]:g["colptr"][i + 1]]
+        rv = g["vals"][g["colptr"][i]:g["colptr"][i + 1]]
+        rvar = g["var"][g["colptr"][i]:g["colptr"][i + 1]]
+        col = np.zeros(nvox)
+        vcol = np.zeros(nvox)
+        col[rows[colptr[i]:colptr[i + 1]]] = vals[colptr[i]:colptr[i + 1]]
+        vcol[rows[colptr[i]:colptr[i + 1]]] = var[colptr[i]:colptr[i + 1]]
+        sel = rv > 0.05 * rv.max()
+        zs.append((col[rr[sel]] - rv[sel]) / np.sqrt(vcol[rr[sel]] + rvar[sel]))
+    z = np.concatenate(zs)
+    assert len(z) > 250
+    assert np.mean(np.abs(z) < 3) >= 0.99, np.mean(np.abs(z) < 3)
+    assert abs(z.mean()) < 0.25
