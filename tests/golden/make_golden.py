@@ -211,10 +211,11 @@ def make_gamma(name, nbatch=100, cores=8):
 DIJ = dict(gantry=[0.0, 90.0], bixel=1.0, field=(2.0, 2.0), nhist=100000, nbatch=10, rel=1e-4)
 
 
-def make_dij():
+def make_dij(gaussian=False):
     """matRad D_ij of the ctsmall phantom from the unmodified MEX entry, one
     call per beamlet (each call starts its sums at zero, so V is the
-    beamlet's own variance of the mean)."""
+    beamlet's own variance of the mean).  gaussian: the Gaussian focal spot
+    (sourceGeometry 'gaussian', width 0.2123 cm) -> dijg_ctsmall.npz."""
     from oracle.ref import matrad_dij
     from ompmc_b200.engine import bixel_grid
     ph = CASES["ctsmall"]["phantom"]()
@@ -225,15 +226,16 @@ def make_dij():
         one = dict(bl, corner=bl["corner"][i:i + 1], side1=bl["side1"][i:i + 1], side2=bl["side2"][i:i + 1],
                    ibeam=bl["ibeam"][i:i + 1])
         jc, ir, pr, var = matrad_dij(ph, one, DIJ["nhist"], DIJ["nbatch"], seeds=(97, 33 + i),
-                                     rel_threshold=DIJ["rel"], spectrum_file=str(spec))
+                                     rel_threshold=DIJ["rel"], spectrum_file=str(spec), gaussian=gaussian)
         nnz_full.append(len(pr))
         keep = pr > 0.01 * pr.max()          # the fixture keeps entries above 1 % of the column maximum
         cols.append((ir[keep], pr[keep], var[keep]))
     colptr = np.concatenate([[0], np.cumsum([len(c[0]) for c in cols])])
-    np.savez_compressed(HERE / "dij_ctsmall.npz", colptr=colptr, rows=np.concatenate([c[0] for c in cols]).astype(np.int32),
+    np.savez_compressed(HERE / ("dijg_ctsmall.npz" if gaussian else "dij_ctsmall.npz"), colptr=colptr, rows=np.concatenate([c[0] for c in cols]).astype(np.int32),
                         vals=np.concatenate([c[1] for c in cols]), var=np.concatenate([c[2] for c in cols]),
                         src=bl["src"], corner=bl["corner"], side1=bl["side1"], side2=bl["side2"], ibeam=bl["ibeam"],
-                        nhist=DIJ["nhist"], nbatch=DIJ["nbatch"], rel=DIJ["rel"], nnz_full=np.array(nnz_full))
+                        nhist=DIJ["nhist"], nbatch=DIJ["nbatch"], rel=DIJ["rel"], nnz_full=np.array(nnz_full),
+                        gaussian=int(gaussian))
 
 
 def main():
@@ -264,6 +266,9 @@ def main():
     if not a.only or a.only in "dij_ctsmall":
         print("generating dij_ctsmall", flush=True)
         make_dij()
+    if not a.only or a.only in "dijg_ctsmall":
+        print("generating dijg_ctsmall", flush=True)
+        make_dij(gaussian=True)
 
 
 if __name__ == "__main__":

@@ -9,10 +9,10 @@ import numpy as np
 import pytest
 
 
-def mex_inputs(assets_root, golden, nhist=None):
+def mex_inputs(assets_root, golden, nhist=None, fixture="dij_ctsmall"):
     from tests.conftest import case_phantom
     ph = case_phantom("ctsmall")
-    g = golden("dij_ctsmall")
+    g = golden(fixture)
     cubeRho = np.ascontiguousarray(ph.rho.transpose(2, 1, 0))        # (nx, ny, nz) MATLAB indexing
     cubeMatIx = np.ascontiguousarray(ph.med.transpose(2, 1, 0)).astype(np.int32)
     mcGeo = dict(material=[[m, ""] for m in ph.media], xBounds=ph.xb, yBounds=ph.yb, zBounds=ph.zb)
@@ -29,6 +29,8 @@ def mex_inputs(assets_root, golden, nhist=None):
                  pgs4formFile=str(assets_root / "pegs4" / "pgs4form.dat"),
                  dataFolder=str(assets_root / "data") + "/", outputFolder=str(assets_root / "out") + "/",
                  relDoseThreshold=float(g["rel"]))
+    if int(g.get("gaussian", 0)):
+        mcOpt.update(sourceGeometry="gaussian", sourceGaussianWidth=0.2123)
     return cubeRho, cubeMatIx, mcGeo, mcSrc, mcOpt
 
 
@@ -61,10 +63,12 @@ def test_too_many_outputs(assets_root, golden):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("transport", ["event", "plain"])
-def test_mirror_matches_matrad_reference(transport, assets_root, golden):
+@pytest.mark.parametrize("fixture", ["dij_ctsmall", "dijg_ctsmall"], ids=["point", "gaussian"])
+def test_mirror_matches_matrad_reference(fixture, transport, assets_root, golden):
+    """dijg: the Gaussian focal spot (omc_matrad.c:1252-1295)."""
     from ompmc_b200.matrad import matrad_dij
-    g = golden("dij_ctsmall")
-    args = mex_inputs(assets_root, golden)
+    g = golden(fixture)
+    args = mex_inputs(assets_root, golden, fixture=fixture)
     args[4]["transport"] = transport
     D, V = matrad_dij(*args, nargout=2)
     nvox = int(np.prod(args[0].shape))
