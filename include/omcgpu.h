@@ -102,6 +102,10 @@ typedef struct {
                              sampled physics is the same; default 2; 0 = the
                              reference's restart after every step, which
                              also costs a zero-length step each time) */
+    int electron_interact_kernel; /* event form: 1 (default) = electrons'
+                             discrete interactions are sampled in a kernel of
+                             their own after the transport kernel (0 = in
+                             place); results do not depend on it */
 } omc_options;
 
 void omc_options_default(omc_options *o);

@@ -97,6 +97,8 @@ struct DevData {
     int chsteps;                     // electrons: condensed-history steps after which the
                                      // distance to the next discrete interaction is re-drawn
                                      // (0 = the reference's restart after every step)
+    int defer_interact;              // electrons: leave discrete interactions to a separate
+                                     // kernel (event form) instead of sampling them in place
 };
 
 // Beam source of the dosxyz ucode (omc_dosxyz.c:337-632, :964-1068).

@@ -199,6 +199,7 @@ static int build_devset(omc_engine *e, DevSet<R> &S) {
     // trajectories replay the reference's); the event form re-draws after
     // electron_chsteps steps
     d.chsteps = sizeof(R) == 4 ? std::max(0, e->opt.electron_chsteps) : 0;
+    d.defer_interact = sizeof(R) == 4 ? (e->opt.electron_interact_kernel ? 1 : 0) : 0;
     d.xb = S.xb.template as<R>(); d.yb = S.yb.template as<R>(); d.zb = S.zb.template as<R>();
     d.med = S.med.template as<int8_t>(); d.rhof = S.rhof.template as<R>();
     d.ms = S.ms.template as<MedS<R>>(); d.ph = S.ph.template as<PhBin<R>>(); d.pmax = S.pmax.template as<PL<R>>();
@@ -481,6 +482,7 @@ void omc_options_default(omc_options *o) {
     o->nsplit = 1;
     o->electron_split = 0.3;
     o->electron_chsteps = 2;
+    o->electron_interact_kernel = 1;
 }
 
 int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_options *o, omc_engine **out) {

@@ -30,6 +30,7 @@ struct Queue {
 struct Ctl {
     int cnt[4];               // photon A, electron A, photon B, electron B (from the bottom)
     int cnt_hi[4];            // the same queues, entries from the top
+    int cnt_int, cnt_int_hi;  // electrons waiting for their discrete interaction (this cycle)
     long long hist_next;      // next history to inject
     long long hist_total;     // histories requested
     int inject;               // histories injected this cycle
@@ -40,7 +41,8 @@ struct Ctl {
     double src_energy;        // sum of primary kinetic energies
     int tsteps;               // this cycle's electron budget (tstep-loop iterations per event)
     float esplit;             // regroup energy (total, MeV): electrons above it go to the top
-    int fetch[2];             // work counters of the photon and electron kernels
+    int fetch[3];             // work counters of the photon, electron and interaction kernels
+    int pad3;
     // counters per transport kernel (0 photon, 1 electron)
     unsigned long long st_events[2], st_steps[2], st_cross[2], st_dep[2], st_atom[2];
 };
@@ -67,12 +69,14 @@ struct EventState {
     int cap = 0;              // per queue
     DBuf buf[4];              // photon A, electron A, photon B, electron B (13 arrays each)
     DBuf split_buf[2];        // splitting state of the photon queues (nsplit > 1)
+    DBuf int_buf;             // electrons at their discrete interaction (defer_interact)
+    Queue qi;
     Queue q[4];
     DBuf ctl;
     Ctl *ctl_d = nullptr;
     int block = 256;
     int grid = 0;             // source kernels
-    int grid_p = 0, grid_e = 0;  // transport kernels: one wave of resident blocks
+    int grid_p = 0, grid_e = 0, grid_i = 0;  // transport kernels: one wave of resident blocks
     int lanes = 0;            // resident threads of the electron kernel
     int boost = 32;           // budget multiplier limit in the drain tail
     int tsteps = 2;           // electron tstep iterations per event launch
@@ -113,6 +117,7 @@ struct ServeDev {
 };
 
 int event_prepare(omc_engine *e);
+int event_interact_queue(omc_engine *e);
 // One serving cycle with input buffers `in` (0 = A, 1 = B); tally slot of a
 // particle = request slot * nbmax + batch.
 void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);

@@ -1237,7 +1237,7 @@ OMC_OUTLINE R eloss(const DevData<R> &D, int imed, int qel, R rhof, R tustep, R 
 }
 
 // ------------------------------------------------------- electron step
-enum EStep : int { E_DEAD = 0, E_ALIVE = 1 };
+enum EStep : int { E_DEAD = 0, E_ALIVE = 1, E_INTERACT = 2 };
 
 // Electron/positron below its cut-off: deposit the kinetic energy; a
 // positron annihilates at rest (ompmc.c:4683-4705 and repeats).
@@ -1250,6 +1250,49 @@ OMC_COLD int e_cutoff(const DevData<R> &D, Env &g, Part<R> &p, R eie) {
         return E_ALIVE;
     }
     return E_DEAD;
+}
+
+// The discrete interaction at the end of electron()'s transport loop
+// (ompmc.c:5300-5451): bremsstrahlung or Moller (e-), bremsstrahlung,
+// Bhabha or annihilation in flight (e+), by the branching ratios at the
+// particle's energy (elke = ln of its kinetic energy, lelke its bin).
+template <typename R, typename Env>
+OMC_HD void electron_interact_at(const DevData<R> &D, Env &g, Part<R> &p, int imed, int qel, R elke, int lelke) {
+    const ElBin<R> &B = ebin(D, imed, qel, lelke);
+    if (p.iq < 0) {
+        R ebr1 = pwl(B.br1, elke);
+        R rnno = g.uni();
+        if (rnno <= ebr1) {
+            brems(D, g, p);
+        } else if (p.e <= D.ms[imed].thmoll) {
+            if (ebr1 <= R(0)) return;
+            brems(D, g, p);
+        } else {
+            moller(D, g, p);
+        }
+    } else {
+        R pbr1 = pwl(B.br1, elke);
+        R rnno = g.uni();
+        if (rnno < pbr1) {
+            brems(D, g, p);
+        } else {
+            R pbr2 = pwl(B.br2, elke);
+            if (rnno < pbr2) bhabha(D, g, p);
+            else annih(D, g, p);
+        }
+    }
+}
+
+// The same for a particle left at its interaction site by electron_step
+// (E_INTERACT): medium, energy and bin are recomputed from the particle
+// exactly as the transport loop computed them.
+template <typename R, typename Env>
+OMC_HD void electron_interact(const DevData<R> &D, Env &g, Part<R> &p) {
+    int imed = D.med[p.ir];
+    const MedS<R> &M = D.ms[imed];
+    R elke = m_log(p.e - R(D_RM));
+    int lelke = lidx(M.eke1, M.eke0, elke);
+    electron_interact_at(D, g, p, imed, (1 + p.iq) / 2, elke, lelke);
 }
 
 // One call of electron(): class II condensed-history transport with the
@@ -1521,30 +1564,10 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
         R rfict = g.uni();
         if (!(rfict >= sigratio)) break;
     }
-    // discrete interaction
-    const ElBin<R> &B = ebin(D, imed, qel, lelke);
-    if (iq < 0) {
-        R ebr1 = pwl(B.br1, elke);
-        R rnno = g.uni();
-        if (rnno <= ebr1) {
-            brems(D, g, p);
-        } else if (p.e <= D.ms[imed].thmoll) {
-            if (ebr1 <= R(0)) return E_ALIVE;
-            brems(D, g, p);
-        } else {
-            moller(D, g, p);
-        }
-    } else {
-        R pbr1 = pwl(B.br1, elke);
-        R rnno = g.uni();
-        if (rnno < pbr1) {
-            brems(D, g, p);
-        } else {
-            R pbr2 = pwl(B.br2, elke);
-            if (rnno < pbr2) bhabha(D, g, p);
-            else annih(D, g, p);
-        }
-    }
+    // discrete interaction: here, or (D.defer_interact) in a later kernel
+    // that runs electron_interact on the particle as it stands
+    if (D.defer_interact) return E_INTERACT;
+    electron_interact_at(D, g, p, imed, qel, elke, lelke);
     return E_ALIVE;
 }
 

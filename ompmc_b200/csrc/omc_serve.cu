@@ -313,6 +313,7 @@ int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint6
     *out = nullptr;
     cudaSetDevice(e->device);
     int rc = event_prepare(e);
+    if (!rc) rc = event_interact_queue(e);
     if (rc) return rc;
     auto s = std::make_unique<omc_server>();
     s->e = e;
@@ -570,7 +571,7 @@ int omc_run_beamlets(omc_engine *e, const omc_beamlets *b, int64_t nhist, int nb
             cvar[i] = std::move(r.var);
             histories += r.nhist;
         }
-        launches = (double)s->cycles * 4;
+        launches = (double)s->cycles * (e->d32.d.defer_interact ? 5 : 4);
     } else if (mode == OMC_PLAIN_FP64) {
         PlanBuf pb;
         if ((rc = upload_plan<double>(e, b, pb.f64, pb.s64))) return rc;

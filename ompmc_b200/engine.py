@@ -51,7 +51,7 @@ class _Options(C.Structure):
                 ("ref_compat", C.c_int), ("queue_capacity", C.c_int64), ("block", C.c_int),
                 ("nsplit", C.c_int), ("profile", C.c_int), ("electron_tsteps", C.c_int),
                 ("inflight", C.c_int64), ("tail_boost", C.c_int), ("electron_split", C.c_double),
-                ("electron_chsteps", C.c_int)]
+                ("electron_chsteps", C.c_int), ("electron_interact_kernel", C.c_int)]
 
 
 class _Energy(C.Structure):
@@ -197,7 +197,7 @@ class Engine:
 
     def __init__(self, tables: Tables, phantom, ecut=0.7, pcut=0.01, device=0, ref_compat=True,
                  queue_capacity=0, block=0, profile=False, electron_tsteps=0, inflight=0, tail_boost=0,
-                 electron_split=None, nsplit=1, electron_chsteps=None):
+                 electron_split=None, nsplit=1, electron_chsteps=None, electron_interact_kernel=None):
         L = lib()
         self.tables = tables
         self.phantom = phantom
@@ -225,6 +225,8 @@ class Engine:
             o.electron_split = electron_split
         if electron_chsteps is not None:
             o.electron_chsteps = int(electron_chsteps)
+        if electron_interact_kernel is not None:
+            o.electron_interact_kernel = int(electron_interact_kernel)
         h = C.c_void_p()
         _check(L.omc_engine_create(tables.h, C.byref(P), C.byref(o), C.byref(h)))
         self.h = h

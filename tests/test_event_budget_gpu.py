@@ -17,7 +17,8 @@ pytestmark = pytest.mark.gpu
 
 CONFIGS = {
     "nsplit1": [dict(electron_tsteps=1, tail_boost=1, electron_split=0.0), dict(),
-                dict(electron_tsteps=7, tail_boost=64), dict(electron_split=1.0, block=128, inflight=1 << 18)],
+                dict(electron_tsteps=7, tail_boost=64), dict(electron_split=1.0, block=128, inflight=1 << 18),
+                dict(electron_interact_kernel=1, electron_tsteps=3)],
     # photon splitting: a split photon's state (sub-photon, survivor,
     # stratification offset) is carried from event to event
     "nsplit5": [dict(nsplit=5, electron_tsteps=1, tail_boost=1, electron_split=0.0), dict(nsplit=5),
