@@ -106,6 +106,11 @@ typedef struct {
                              discrete interactions are sampled in a kernel of
                              their own after the transport kernel (0 = in
                              place); results do not depend on it */
+    int photon_woodcock;  /* event form: 1 (default) = photons are tracked by
+                             delta (Woodcock) tracking against the largest
+                             attenuation in the phantom instead of voxel by
+                             voxel, when the grid is uniform (same sampled
+                             distribution) */
 } omc_options;
 
 void omc_options_default(omc_options *o);

@@ -99,6 +99,13 @@ struct DevData {
                                      // (0 = the reference's restart after every step)
     int defer_interact;              // electrons: leave discrete interactions to a separate
                                      // kernel (event form) instead of sampling them in place
+    // photons: delta (Woodcock) tracking on a uniform voxel grid (event form)
+    int woodcock;                    // 1: photons walk by delta tracking, not voxel by voxel
+    int uniform;                     // the grid is uniform on all three axes
+    R gx0, gy0, gz0;                 // lower corner of the grid
+    R gx1, gy1, gz1;                 // upper corner
+    R gidx, gidy, gidz;              // 1 / voxel size per axis
+    R rhomax[D_MXMED];               // largest density ratio of each medium in the phantom
 };
 
 // Beam source of the dosxyz ucode (omc_dosxyz.c:337-632, :964-1068).

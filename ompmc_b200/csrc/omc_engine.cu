@@ -77,6 +77,30 @@ void make_layout(const Tables &t, const Phantom &ph, const Regions &rg, double e
     d.nz = ph.nz;
     d.ref_compat = ref_compat;
     d.nsplit = 1;
+    // uniform grid and per-medium density maxima (photon delta tracking)
+    auto uniform_axis = [](const std::vector<double> &b, double &x0, double &x1, double &inv) {
+        int n = (int)b.size() - 1;
+        x0 = b[0];
+        x1 = b[n];
+        double dx = (x1 - x0) / n;
+        inv = 1.0 / dx;
+        for (int i = 0; i < n; i++)
+            if (std::fabs((b[i + 1] - b[i]) - dx) > 1e-6 * dx) return false;
+        return dx > 0;
+    };
+    double ax[3][3];
+    bool uni = uniform_axis(ph.xb, ax[0][0], ax[0][1], ax[0][2]);
+    uni = uniform_axis(ph.yb, ax[1][0], ax[1][1], ax[1][2]) && uni;
+    uni = uniform_axis(ph.zb, ax[2][0], ax[2][1], ax[2][2]) && uni;
+    d.uniform = uni ? 1 : 0;
+    d.gx0 = (R)ax[0][0]; d.gx1 = (R)ax[0][1]; d.gidx = (R)ax[0][2];
+    d.gy0 = (R)ax[1][0]; d.gy1 = (R)ax[1][1]; d.gidy = (R)ax[1][2];
+    d.gz0 = (R)ax[2][0]; d.gz1 = (R)ax[2][1]; d.gidz = (R)ax[2][2];
+    for (int m = 0; m < D_MXMED; m++) d.rhomax[m] = 0;
+    for (size_t r = 1; r < rg.med.size(); r++) {
+        int m = rg.med[r];
+        if (m >= 0 && m < D_MXMED) d.rhomax[m] = std::max(d.rhomax[m], (R)rg.rhof[r]);
+    }
     L.xb.assign(ph.xb.begin(), ph.xb.end());
     L.yb.assign(ph.yb.begin(), ph.yb.end());
     L.zb.assign(ph.zb.begin(), ph.zb.end());
@@ -200,6 +224,7 @@ static int build_devset(omc_engine *e, DevSet<R> &S) {
     // electron_chsteps steps
     d.chsteps = sizeof(R) == 4 ? std::max(0, e->opt.electron_chsteps) : 0;
     d.defer_interact = sizeof(R) == 4 ? (e->opt.electron_interact_kernel ? 1 : 0) : 0;
+    d.woodcock = sizeof(R) == 4 && d.uniform && e->opt.photon_woodcock ? 1 : 0;
     d.xb = S.xb.template as<R>(); d.yb = S.yb.template as<R>(); d.zb = S.zb.template as<R>();
     d.med = S.med.template as<int8_t>(); d.rhof = S.rhof.template as<R>();
     d.ms = S.ms.template as<MedS<R>>(); d.ph = S.ph.template as<PhBin<R>>(); d.pmax = S.pmax.template as<PL<R>>();
@@ -483,6 +508,7 @@ void omc_options_default(omc_options *o) {
     o->electron_split = 0.3;
     o->electron_chsteps = 2;
     o->electron_interact_kernel = 1;
+    o->photon_woodcock = 1;
 }
 
 int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_options *o, omc_engine **out) {

@@ -358,7 +358,7 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
         bool alive = false, defer = false;
         if (valid) {
             if (KIND == EV_PHOTON) {
-                alive = photon_step(D, g, p);
+                alive = D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p);
             } else if (KIND == EV_ELECTRON) {
                 int r = electron_step(D, g, p);
                 alive = r != E_DEAD;

@@ -595,6 +595,82 @@ OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
     return true;
 }
 
+// Photon event by delta (Woodcock) tracking, for uniform voxel grids (the
+// event form; D.woodcock).  The same physics as photon_step: the distance
+// to the next real interaction is exponential in the local attenuation
+// mu(x) = rhof(x) / (gmfp(E) * cohfac(E)) of the voxel medium, sampled here
+// against the largest attenuation mu_max of the phantom at this energy:
+// tentative steps of -ln(xi)/mu_max, each accepted as a real interaction
+// with probability mu(x)/mu_max (a standard, exact method; Woodcock et
+// al. 1965).  A photon in a 0.25 cm grid then takes a few steps per event
+// instead of one per voxel crossed.  The interaction itself is photon_step's.
+template <typename R, typename Env>
+OMC_HD bool photon_step_delta(const DevData<R> &D, Env &g, Part<R> &p) {
+    R eig = p.e;
+    if (eig <= pcut_of(D, p.ir) || p.wt == R(0)) {
+        g.deposit(p.ir, p.wt * eig);
+        return false;
+    }
+    R gle = m_log(eig);
+    R mu_max = 0;
+    for (int m = 0; m < D.nmed; m++) {
+        const MedS<R> &M = D.ms[m];
+        const PhBin<R> &b = pbin(D, m, lidx(M.ge1, M.ge0, gle));
+        mu_max = m_max(mu_max, D.rhomax[m] / (pwl(b.gmfp, gle) * pwl(b.cohe, gle)));
+    }
+    if (!(mu_max > R(0))) return false;
+    // distance to the grid's boundary along the direction
+    R texit = R(1.0E30);
+    if (p.u > R(0)) texit = m_min(texit, (D.gx1 - p.x) / p.u);
+    else if (p.u < R(0)) texit = m_min(texit, (D.gx0 - p.x) / p.u);
+    if (p.v > R(0)) texit = m_min(texit, (D.gy1 - p.y) / p.v);
+    else if (p.v < R(0)) texit = m_min(texit, (D.gy0 - p.y) / p.v);
+    if (p.w > R(0)) texit = m_min(texit, (D.gz1 - p.z) / p.w);
+    else if (p.w < R(0)) texit = m_min(texit, (D.gz0 - p.z) / p.w);
+    const R x0 = p.x, y0 = p.y, z0 = p.z;
+    const R inv_mu = R(1) / mu_max;
+    R t = 0;
+    int imed = -1, lgle = 0;
+    R cohfac = 0;
+    for (int guard = 0;; guard++) {
+        if (guard > 100000 || !g.tick()) {
+            g.err(ERR_LOOP);
+            return false;
+        }
+        t += -m_log(R(1) - g.uni()) * inv_mu;
+        if (t >= texit) return false;   // leaves the phantom
+        R x = x0 + t * p.u, y = y0 + t * p.v, z = z0 + t * p.w;
+        int i = min(max((int)((x - D.gx0) * D.gidx), 0), D.nx - 1);
+        int j = min(max((int)((y - D.gy0) * D.gidy), 0), D.ny - 1);
+        int k = min(max((int)((z - D.gz0) * D.gidz), 0), D.nz - 1);
+        int ir = 1 + i + D.nx * (j + D.ny * k);
+        int m = D.med[ir];
+        R r = g.uni();
+        if (m < 0) continue;
+        const MedS<R> &M = D.ms[m];
+        int l = lidx(M.ge1, M.ge0, gle);
+        const PhBin<R> &b = pbin(D, m, l);
+        R coh = pwl(b.cohe, gle);
+        R mu = D.rhof[ir] / (pwl(b.gmfp, gle) * coh);
+        if (r * mu_max <= mu) {
+            p.x = x; p.y = y; p.z = z;
+            if (ir != p.ir) g.cross();
+            p.ir = ir;
+            imed = m;
+            lgle = l;
+            cohfac = coh;
+            break;
+        }
+    }
+    R rnno = g.uni();
+    if (rnno <= R(1) - cohfac) {
+        rayleigh(D, g, p, imed, gle, lgle);
+        return true;
+    }
+    photon_interact(D, g, p, eig, gle, imed, lgle);
+    return true;
+}
+
 // Russian roulette of a photon made by an electron interaction when photons
 // are split (ompmc.c:4169-4182, 4358-4371, 4647-4660): it survives with
 // probability 1/nsplit and then carries nsplit times its weight; otherwise
