@@ -38,6 +38,9 @@ constexpr int EV_MAXOUT = 1;       // secondaries an event emits: every interact
 constexpr int EV_MAXOUT_SPLIT = 2; // products of a split photon's sub-photon (pair: two)
 constexpr int EV_MAX_BLOCK = 256;  // launch bound of the transport kernels
 
+using TransportKernel = void (*)(DevData<float>, Queue, Queue, Queue, double *, long, Ctl *, uint32_t, int *, int,
+                                 Queue);
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -312,14 +315,15 @@ __device__ __forceinline__ bool split_event(const DevData<float> &D, Env &g, Par
 // or EV_INTERACT (electrons at their discrete interaction, with
 // D.defer_interact).  `qi`: the interaction queue (EV_ELECTRON with
 // D.defer_interact appends there).
-enum { EV_PHOTON = 0, EV_ELECTRON = 1, EV_SPLIT = 2, EV_INTERACT = 3 };
+enum { EV_PHOTON = 0, EV_ELECTRON = 1, EV_SPLIT = 2, EV_INTERACT = 3, EV_ELECTRON_DEFER = 4 };
 template <int KIND>
 __device__ __forceinline__ void transport_events(const DevData<float> &D, const Queue &in, const Queue &outP,
                                                  const Queue &outE, double *tallies, long nvox, Ctl *ctl,
                                                  uint32_t seedw, int *live, int nbmax, const Queue &qi) {
     constexpr int MAXOUT = KIND == EV_SPLIT ? EV_MAXOUT_SPLIT : EV_MAXOUT;
     const unsigned full = 0xffffffffu;
-    const int kq = KIND == EV_ELECTRON ? 1 : (KIND == EV_INTERACT ? 2 : 0);
+    constexpr bool ELECTRON = KIND == EV_ELECTRON || KIND == EV_ELECTRON_DEFER;
+    const int kq = ELECTRON ? 1 : (KIND == EV_INTERACT ? 2 : 0);
     const int ks = KIND == EV_PHOTON || KIND == EV_SPLIT ? 0 : 1;   // counters: photon or electron
     const int n = queue_size(in);
     const int tsteps = ctl->tsteps;
@@ -359,8 +363,8 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
         if (valid) {
             if (KIND == EV_PHOTON) {
                 alive = D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p);
-            } else if (KIND == EV_ELECTRON) {
-                int r = electron_step(D, g, p);
+            } else if (ELECTRON) {
+                int r = electron_step<float, EvEnv<MAXOUT>, KIND == EV_ELECTRON_DEFER>(D, g, p);
                 alive = r != E_DEAD;
                 defer = r == E_INTERACT;
             } else if (KIND == EV_SPLIT) {
@@ -371,7 +375,7 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
             }
             g.flush();
         }
-        int emitted = KIND == EV_ELECTRON
+        int emitted = KIND == EV_ELECTRON_DEFER
                           ? emit<MAXOUT, true>(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr, &qi, defer)
                           : emit(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr);
         if (live) add_live(live, nbmax, valid ? slot : 0, valid ? emitted - 1 : 0, full);
@@ -410,10 +414,18 @@ __global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_split_step(DevData<floa
 // re-queued.  Four resident blocks of 256 threads per SM (64 registers,
 // a few spills) measured faster than three (80) or two (114): the step is
 // latency bound and more warps hide more of it.
+template <bool DEFER>
 __global__ void __launch_bounds__(EV_MAX_BLOCK, 4) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
                                                        double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
                                                        int *live, int nbmax, Queue qi) {
-    transport_events<EV_ELECTRON>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax, qi);
+    transport_events<DEFER ? EV_ELECTRON_DEFER : EV_ELECTRON>(D, in, outP, outE, tallies, nvox, ctl, seedw, live,
+                                                               nbmax, qi);
+}
+
+// The electron kernel of the engine: interactions in a kernel of their own
+// (D.defer_interact) or in place.
+static TransportKernel electron_kernel(const omc_engine *e) {
+    return e->d32.d.defer_interact ? k_electron_step<true> : k_electron_step<false>;
 }
 
 // Discrete interactions of the electrons the electron kernel left at their
@@ -526,9 +538,6 @@ static int alloc_queue(omc_engine *e, DBuf &b, Queue &q, int cap, int *count, in
     return OMC_OK;
 }
 
-using TransportKernel = void (*)(DevData<float>, Queue, Queue, Queue, double *, long, Ctl *, uint32_t, int *, int,
-                                 Queue);
-
 // The photon kernel of the engine: split photons when nsplit > 1.
 static TransportKernel photon_kernel(const omc_engine *e) {
     return e->d32.d.nsplit > 1 ? k_photon_split_step : k_photon_step;
@@ -538,7 +547,7 @@ static TransportKernel photon_kernel(const omc_engine *e) {
 static void size_grids(omc_engine *e, EventState &S) {
     int bp = 0, be = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, photon_kernel(e), S.block, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, k_electron_step, S.block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, electron_kernel(e), S.block, 0);
     S.grid_p = e->sm_count * std::max(1, bp);
     S.grid_e = e->sm_count * std::max(1, be);
     int bi = 0;
@@ -650,7 +659,7 @@ static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, doubl
     photon_kernel(e)<<<S.grid_p, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
                                                             S.ctl_d, seedw, nullptr, 1, S.qi);
     if (ev) cudaEventRecord(ev[3], e->stream);
-    k_electron_step<<<S.grid_e, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
+    electron_kernel(e)<<<S.grid_e, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
                                                              S.ctl_d, seedw, nullptr, 1, S.qi);
     if (e->d32.d.defer_interact)
         k_electron_interact<<<S.grid_i, S.block, 0, e->stream>>>(e->d32.d, S.qi, S.q[oph], S.q[oel], tallies, nvox,
@@ -892,7 +901,7 @@ void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, in
     k_serve_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, sd, S.q[iph], S.q[iel], S.ctl_d, nbmax, seedw);
     photon_kernel(e)<<<S.grid_p, S.block, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
                                                         S.ctl_d, seedw, sd->live, nbmax, S.qi);
-    k_electron_step<<<S.grid_e, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
+    electron_kernel(e)<<<S.grid_e, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
                                                           S.ctl_d, seedw, sd->live, nbmax, S.qi);
     if (e->d32.d.defer_interact)
         k_electron_interact<<<S.grid_i, S.block, 0, e->stream>>>(e->d32.d, S.qi, S.q[oph], S.q[oel], tallies, nvox,

@@ -1375,8 +1375,9 @@ OMC_HD void electron_interact(const DevData<R> &D, Env &g, Part<R> &p) {
 // fictitious cross-section method until the next discrete interaction, the
 // cut-off or the phantom exit; then the interaction (electron,
 // ompmc.c:4666-5451).  Returns E_ALIVE when p (possibly changed into another
-// particle) stays on the stack.
-template <typename R, typename Env>
+// particle) stays on the stack; with DEFER, E_INTERACT when p stands at its
+// discrete interaction (electron_interact samples it).
+template <typename R, typename Env, bool DEFER = false>
 OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
     const R RMr = R(D_RM);
     int irl = p.ir;
@@ -1640,9 +1641,9 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
         R rfict = g.uni();
         if (!(rfict >= sigratio)) break;
     }
-    // discrete interaction: here, or (D.defer_interact) in a later kernel
-    // that runs electron_interact on the particle as it stands
-    if (D.defer_interact) return E_INTERACT;
+    // discrete interaction: here, or (DEFER) in a later kernel that runs
+    // electron_interact on the particle as it stands
+    if (DEFER) return E_INTERACT;
     electron_interact_at(D, g, p, imed, qel, elke, lelke);
     return E_ALIVE;
 }
