@@ -111,6 +111,13 @@ typedef struct {
                              attenuation in the phantom instead of voxel by
                              voxel, when the grid is uniform (same sampled
                              distribution) */
+    int64_t drain_particles; /* event form: once every history is injected and
+                             at most this many particles are left, they are
+                             run to the end of their sub-histories in one
+                             launch instead of further cycles (0 = default,
+                             half the drain kernel's resident threads;
+                             -1 = never);
+                             results do not depend on it */
 } omc_options;
 
 void omc_options_default(omc_options *o);

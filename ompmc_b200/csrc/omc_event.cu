@@ -13,7 +13,8 @@
 //               own keeps the samplers' code out of the transport kernel's
 //               instruction cache: 8 % faster on slab64)
 // Queues are double-buffered (A -> B, then B -> A), so two cycles form an
-// idempotent CUDA graph that the host replays until every history is done.
+// idempotent CUDA graph that the host replays until every history is
+// injected and few particles are left; k_drain then runs those to the end.
 //
 // An event transports its particle until the next interaction, death or,
 // for electrons, the end of the cycle's budget of tstep-loop iterations.
@@ -437,6 +438,111 @@ __global__ void __launch_bounds__(EV_MAX_BLOCK) k_electron_interact(DevData<floa
     transport_events<EV_INTERACT>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax, qi);
 }
 
+// ------------------------------------------------------------ drain
+// Once every history is injected and few particles remain, transport
+// cycles launch mostly idle kernels whose duration is the latency of their
+// longest events, and each particle waits a whole cycle between events.
+// The drain runs each remaining particle to the end of its sub-history in
+// one launch instead: one thread per queued particle, its secondaries on a
+// local stack.  Every particle keeps its own random stream and its
+// secondaries get the keys emit() gives them, electrons run to their
+// interaction without a budget (budgets do not change trajectories) and
+// interactions are sampled in place (the same draws as the interaction
+// kernel), so the dose is the one the cycles would have produced, up to
+// the summation order of the FP64 tallies.  Not used with photon
+// splitting.
+constexpr int DRAIN_STACK = 48;
+constexpr int DRAIN_BLOCK = 128;
+
+struct DrainPart {
+    Part<float> p;
+    uint32_t k0, k1, pos;
+};
+
+__global__ void __launch_bounds__(DRAIN_BLOCK) k_drain(DevData<float> D, Queue qP, Queue qE, double *tallies,
+                                                        long nvox, Ctl *ctl, uint32_t seedw) {
+    const int np = queue_size(qP), ne = queue_size(qE);
+    const int n = np + ne;
+    DrainPart st[DRAIN_STACK];
+    unsigned flags = 0;
+    unsigned long long c_ev[2] = {0, 0}, c_steps[2] = {0, 0}, c_cross[2] = {0, 0}, c_dep[2] = {0, 0},
+                       c_atom[2] = {0, 0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const Queue &q = t < np ? qP : qE;
+        int tag = 0;
+        qload(q, queue_index(q, t < np ? t : t - np), st[0].p, tag, st[0].k0, st[0].k1, st[0].pos);
+        EvEnv<EV_MAXOUT> g;
+        g.tally = tallies + (long)(tag >> 2) * nvox;
+        g.pend_ir = -1;
+        g.pend_e = 0.0;
+        g.flags = 0;
+        g.natom = 0;
+        int top = 0;
+        for (int guard = 0; top >= 0; guard++) {
+            if (guard > (1 << 22)) {
+                g.flags |= ERR_LOOP;
+                break;
+            }
+            DrainPart &e = st[top];
+            Part<float> p = e.p;
+            const uint64_t pkey = ((uint64_t)e.k1 << 32) | e.k0;
+            g.rng.init(pkey, seedw, e.pos);
+            g.nout = 0;
+            g.work = 0;
+            g.tleft = 1 << 30;
+            g.ncross = g.ndep = 0;
+            const int kind = p.iq == 0 ? 0 : 1;
+            bool alive = kind == 0 ? (D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p))
+                                   : electron_step<float, EvEnv<EV_MAXOUT>, false>(D, g, p) == E_ALIVE;
+            c_ev[kind]++;
+            c_steps[kind] += g.work;
+            c_cross[kind] += g.ncross;
+            c_dep[kind] += g.ndep;
+            if (alive && !(p.e == p.e && p.x == p.x && p.u == p.u)) {
+                g.flags |= ERR_NAN;
+                alive = false;
+            }
+            if (alive && p.iq == 0 && p.wt == 0.f) alive = false;
+            if (alive) {
+                e.p = p;
+                e.pos = g.rng.position();
+            } else {
+                top--;
+            }
+            for (int k = 0; k < g.nout; k++) {
+                const Part<float> &s2 = g.out[k];
+                if (!(s2.e == s2.e && s2.x == s2.x && s2.u == s2.u)) {
+                    g.flags |= ERR_NAN;
+                    continue;
+                }
+                if (s2.iq == 0 && s2.wt == 0.f) continue;
+                if (top + 1 >= DRAIN_STACK) {
+                    g.flags |= ERR_STACK;
+                    continue;
+                }
+                uint64_t ck = mix64(pkey * 0x9E3779B97F4A7C15ull + ((uint64_t)g.out_pos[k] << 1) + 1u +
+                                    ((uint64_t)k << 40));
+                top++;
+                st[top].p = s2;
+                st[top].k0 = (uint32_t)ck;
+                st[top].k1 = (uint32_t)(ck >> 32);
+                st[top].pos = 0;
+            }
+        }
+        g.flush();
+        c_atom[1] += g.natom;     // tally atomics of the whole sub-history
+        flags |= g.flags;
+    }
+    if (flags) atomicOr(&ctl->flags, flags);
+    for (int k = 0; k < 2; k++) {
+        if (c_ev[k]) atomicAdd(&ctl->st_events[k], c_ev[k]);
+        if (c_steps[k]) atomicAdd(&ctl->st_steps[k], c_steps[k]);
+        if (c_cross[k]) atomicAdd(&ctl->st_cross[k], c_cross[k]);
+        if (c_dep[k]) atomicAdd(&ctl->st_dep[k], c_dep[k]);
+        if (c_atom[k]) atomicAdd(&ctl->st_atom[k], c_atom[k]);
+    }
+}
+
 __global__ void k_source(DevData<float> D, BeamSrc<float> S, Queue qP, Queue qE, Ctl *ctl, long long nper,
                          uint64_t seed, uint32_t seedw) {
     int n = ctl->inject;
@@ -550,9 +656,11 @@ static void size_grids(omc_engine *e, EventState &S) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, electron_kernel(e), S.block, 0);
     S.grid_p = e->sm_count * std::max(1, bp);
     S.grid_e = e->sm_count * std::max(1, be);
-    int bi = 0;
+    int bi = 0, bd = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_electron_interact, S.block, 0);
     S.grid_i = e->sm_count * std::max(1, bi);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_drain, DRAIN_BLOCK, 0);
+    S.drain_lanes = e->sm_count * std::max(1, bd) * DRAIN_BLOCK;
     S.lanes = S.grid_e * S.block;
 }
 
@@ -667,6 +775,26 @@ static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, doubl
     if (ev) cudaEventRecord(ev[4], e->stream);
 }
 
+// Particles left in the queues at or below which the transport switches
+// from cycles to the drain (0: never).  By default half the drain kernel's
+// resident threads: the drain serialises each particle's whole remaining
+// cascade in one thread, so it pays only once the cycles are mostly idle
+// (measured on slab64: 40 k best of 5 k - 1 M particles, +11 %).
+static long long drain_threshold(const omc_engine *e) {
+    const EventState &S = *e->ev;
+    if (e->d32.d.nsplit > 1 || e->opt.drain_particles < 0) return 0;
+    return e->opt.drain_particles > 0 ? e->opt.drain_particles : S.drain_lanes / 2;
+}
+
+// The drain over the queues `iph`/`iph + 1` holding `left` particles.
+static void launch_drain(omc_engine *e, int iph, long long left, double *tallies, uint64_t seed) {
+    EventState &S = *e->ev;
+    long long g = (left + DRAIN_BLOCK - 1) / DRAIN_BLOCK;
+    g = std::max(1LL, std::min(g, (long long)S.drain_lanes / DRAIN_BLOCK * 4));
+    k_drain<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[iph + 1], tallies, e->ph.nvox(), S.ctl_d,
+                                                   (uint32_t)(seed >> 32));
+}
+
 // Profiled transport: cycles launched one by one with events around each
 // kernel; per-kernel device time accumulated into S.prof, one trace row per
 // cycle.
@@ -703,6 +831,21 @@ static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallie
         S.prof[2].launches += 1;
         if (h.hist_next >= h.hist_total && cnt_in[0] == 0 && cnt_in[1] == 0) break;
         if (h.flags & ERR_QUEUE) break;
+        long long dthr = drain_threshold(e);
+        if (dthr > 0 && h.hist_next >= h.hist_total && cnt_in[0] + cnt_in[1] <= dthr) {
+            cudaEventRecord(ev[0], e->stream);
+            launch_drain(e, oph, (long long)cnt_in[0] + cnt_in[1], tallies, seed);
+            cudaEventRecord(ev[1], e->stream);
+            if ((rc = cuda_check(e, cudaEventSynchronize(ev[1]), "drain"))) break;
+            float td = 0;
+            cudaEventElapsedTime(&td, ev[0], ev[1]);
+            double row2[6] = {0.0, (double)cnt_in[0], (double)cnt_in[1], 0.0, 0.0, (double)td};
+            S.trace.insert(S.trace.end(), row2, row2 + 6);
+            S.prof[2].seconds += td * 1e-3;
+            S.prof[2].launches += 1;
+            cudaMemcpy(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
+            break;
+        }
         if (cycles > 200000) {
             rc = set_err(e, OMC_E_DEVICE, "event transport did not drain");
             break;
@@ -754,7 +897,7 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
         cudaEventDestroy(t0);
         cudaEventDestroy(t1);
         ks.seconds = ms * 1e-3;
-        ks.launches = cycles * (e->d32.d.defer_interact ? 5 : 4) + nbatch;
+        ks.launches = cycles * (e->d32.d.defer_interact ? 5 : 4) + nbatch + (drain_threshold(e) > 0 ? 1 : 0);
         ks.flags |= h.flags;
         for (int k = 0; k < 2; k++) {
             KernelProfile &P = S.prof[1 + k];
@@ -788,6 +931,8 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
     Ctl h{};
     long graphs = 0;
     int per_check = 4;
+    const long long dthr = drain_threshold(e);
+    int drains = 0;
     for (;;) {
         for (int k = 0; k < per_check; k++) cudaGraphLaunch(exec, e->stream);
         graphs += per_check;
@@ -798,6 +943,21 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
             h.cnt_hi[1] == 0)
             break;
         if (h.flags & ERR_QUEUE) break;
+        if (dthr > 0 && h.hist_next >= h.hist_total) {
+            // every history is in: drain once few particles are left,
+            // checking after every graph until then
+            long long left = (long long)std::min(h.cnt[0] + h.cnt_hi[0], S.cap) +
+                             std::min(h.cnt[1] + h.cnt_hi[1], S.cap);
+            if (left <= dthr) {
+                launch_drain(e, 0, left, tal.as<double>(), seed);
+                drains = 1;
+                if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "drain"))) break;
+                cudaMemcpy(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
+                break;
+            }
+            per_check = 1;
+            continue;
+        }
         // every cycle advances each queued particle by one event, so a run
         // needs (histories / injection rate) + (longest history) cycles
         if (graphs > 50000 + h.hist_total / 1000) {
@@ -814,7 +974,7 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
     float ms = 0;
     cudaEventElapsedTime(&ms, t0, t1);
     ks.seconds = ms * 1e-3;
-    ks.launches = graphs * (e->d32.d.defer_interact ? 10 : 8) + nbatch;
+    ks.launches = graphs * (e->d32.d.defer_interact ? 10 : 8) + nbatch + drains;
     ks.flags |= h.flags;
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);

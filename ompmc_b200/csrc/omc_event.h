@@ -78,6 +78,7 @@ struct EventState {
     int grid = 0;             // source kernels
     int grid_p = 0, grid_e = 0, grid_i = 0;  // transport kernels: one wave of resident blocks
     int lanes = 0;            // resident threads of the electron kernel
+    int drain_lanes = 0;      // resident threads of the drain kernel
     int boost = 32;           // budget multiplier limit in the drain tail
     int tsteps = 2;           // electron tstep iterations per event launch
     double esplit = 0;        // regroup energy of the electron queues (total, MeV)

@@ -52,7 +52,7 @@ class _Options(C.Structure):
                 ("nsplit", C.c_int), ("profile", C.c_int), ("electron_tsteps", C.c_int),
                 ("inflight", C.c_int64), ("tail_boost", C.c_int), ("electron_split", C.c_double),
                 ("electron_chsteps", C.c_int), ("electron_interact_kernel", C.c_int),
-                ("photon_woodcock", C.c_int)]
+                ("photon_woodcock", C.c_int), ("drain_particles", C.c_int64)]
 
 
 class _Energy(C.Structure):
@@ -199,7 +199,7 @@ class Engine:
     def __init__(self, tables: Tables, phantom, ecut=0.7, pcut=0.01, device=0, ref_compat=True,
                  queue_capacity=0, block=0, profile=False, electron_tsteps=0, inflight=0, tail_boost=0,
                  electron_split=None, nsplit=1, electron_chsteps=None, electron_interact_kernel=None,
-                 photon_woodcock=None):
+                 photon_woodcock=None, drain_particles=None):
         L = lib()
         self.tables = tables
         self.phantom = phantom
@@ -231,6 +231,8 @@ class Engine:
             o.electron_interact_kernel = int(electron_interact_kernel)
         if photon_woodcock is not None:
             o.photon_woodcock = int(photon_woodcock)
+        if drain_particles is not None:
+            o.drain_particles = int(drain_particles)
         h = C.c_void_p()
         _check(L.omc_engine_create(tables.h, C.byref(P), C.byref(o), C.byref(h)))
         self.h = h

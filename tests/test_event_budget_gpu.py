@@ -7,8 +7,11 @@ a cycle cuts a particle's transport is invisible in its trajectory.  The
 dose of a run with the smallest fixed budgets (one photon interaction, one
 electron tstep-loop iteration per event) equals the dose with the adaptive
 drain-tail budgets, with large fixed ones and with the electron queues
-regrouped by energy, smaller blocks and fewer particles in flight, up to the
-summation order of the FP64 tally atomics (rtol 1e-9 per voxel)."""
+regrouped by energy, smaller blocks and fewer particles in flight, with the
+interactions sampled in their own kernel and with the remaining particles
+run to completion by the drain kernel at any point after the last
+injection, up to the summation order of the FP64 tally atomics (rtol 1e-9
+per voxel)."""
 import numpy as np
 import pytest
 
@@ -18,7 +21,9 @@ pytestmark = pytest.mark.gpu
 CONFIGS = {
     "nsplit1": [dict(electron_tsteps=1, tail_boost=1, electron_split=0.0), dict(),
                 dict(electron_tsteps=7, tail_boost=64), dict(electron_split=1.0, block=128, inflight=1 << 18),
-                dict(electron_interact_kernel=1, electron_tsteps=3)],
+                dict(electron_interact_kernel=1, electron_tsteps=3),
+                # the drain: never, and as early as every history is in
+                dict(drain_particles=-1), dict(drain_particles=1 << 22)],
     # photon splitting: a split photon's state (sub-photon, survivor,
     # stratification offset) is carried from event to event
     "nsplit5": [dict(nsplit=5, electron_tsteps=1, tail_boost=1, electron_split=0.0), dict(nsplit=5),
