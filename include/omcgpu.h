@@ -128,12 +128,12 @@ int omc_engine_create(const omc_tables *t, const omc_phantom *ph, const omc_opti
 int omc_engine_destroy(omc_engine *e);
 /* Event-form tuning parameters of a live engine (the options of the same
  * names; a value <= 0 keeps the current one, for electron_split and
- * electron_chsteps a value < 0).  Dose does not depend on the first five
- * (up to the summation order of the FP64 tallies) and its distribution
- * not on electron_chsteps; the autotuner (ompmc_b200/autotune.py) sweeps
- * them. */
+ * electron_chsteps a value < 0, for drain_particles -2).  Dose does not
+ * depend on them (up to the summation order of the FP64 tallies) except
+ * electron_chsteps, on which its distribution does not depend; the
+ * autotuner (ompmc_b200/autotune.py) sweeps them. */
 int omc_event_params(omc_engine *e, int electron_tsteps, int tail_boost, int64_t inflight, int block,
-                     double electron_split, int electron_chsteps);
+                     double electron_split, int electron_chsteps, int64_t drain_particles);
 const char *omc_engine_last_error(const omc_engine *e);
 
 /* Per-kernel profile of the last event-form omc_run_beam made with

@@ -14,7 +14,9 @@ for speed per phantom, source and GPU:
 * electron_split  — regroup energy: electrons above it (kinetic, MeV) are
                     queued apart from the others (0 = one group);
 * electron_chsteps — condensed-history steps between re-draws of an
-                    electron's distance to its next discrete interaction.
+                    electron's distance to its next discrete interaction;
+* drain_particles — particles left at which the run switches from cycles
+                    to the drain kernel (-1 never, 0 default).
 
 `tune_beam` runs short dose runs of the given beam on a live engine and
 searches the space coordinate by coordinate (each parameter swept with the
@@ -35,9 +37,10 @@ SPACE = {
     "block": [64, 128, 256],
     "electron_split": [0.0, 0.2, 0.3, 0.5, 1.0],
     "electron_chsteps": [1, 2, 4, 8],
+    "drain_particles": [-1, 10000, 20000, 40000, 80000],
 }
 DEFAULT = {"electron_tsteps": 1, "tail_boost": 32, "inflight": 1 << 20, "block": 256, "electron_split": 0.3,
-           "electron_chsteps": 2}
+           "electron_chsteps": 2, "drain_particles": 0}
 
 
 def _rate(eng, cfg, nhist, run_kw, repeats):

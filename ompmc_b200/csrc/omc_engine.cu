@@ -583,9 +583,10 @@ int omc_engine_destroy(omc_engine *e) {
 const char *omc_engine_last_error(const omc_engine *e) { return e ? e->err.c_str() : omc_last_error(); }
 
 int omc_event_params(omc_engine *e, int electron_tsteps, int tail_boost, int64_t inflight, int block,
-                     double electron_split, int electron_chsteps) {
+                     double electron_split, int electron_chsteps, int64_t drain_particles) {
     if (!e) return global_err(OMC_E_ARG, "omc_event_params: null engine");
     cudaSetDevice(e->device);
+    if (drain_particles >= -1) e->opt.drain_particles = drain_particles;
     if (electron_chsteps >= 0) {
         e->opt.electron_chsteps = electron_chsteps;
         e->d32.d.chsteps = electron_chsteps;

@@ -103,7 +103,8 @@ def lib():
         "omc_dosxyz_run": ([C.c_char_p, C.c_char_p, C.c_int, C.c_int], C.c_int),
         "omc_profile_last": ([C.c_void_p, _dp, C.c_int], C.c_int),
         "omc_profile_trace": ([C.c_void_p, _dp, C.c_int], C.c_int),
-        "omc_event_params": ([C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int, C.c_double, C.c_int], C.c_int),
+        "omc_event_params": ([C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int, C.c_double, C.c_int, C.c_int64],
+                             C.c_int),
         "omc_run_beam_noalloc": ([C.c_void_p, C.POINTER(_Beam), C.c_int64, C.c_int, C.c_uint64, _dp, _dp, _dp],
                                  C.c_int),
         "omc_server_create": ([C.c_void_p, C.c_int64, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)], C.c_int),
@@ -361,11 +362,11 @@ class Engine:
 
     # ------------------------------------------------ validation hooks
     def event_params(self, electron_tsteps=0, tail_boost=0, inflight=0, block=0, electron_split=-1.0,
-                     electron_chsteps=-1):
+                     electron_chsteps=-1, drain_particles=-2):
         """Event-form tuning parameters (0, or -1 for electron_split and
-        electron_chsteps, keeps the current value)."""
+        electron_chsteps, -2 for drain_particles, keeps the current value)."""
         _check(lib().omc_event_params(self.h, int(electron_tsteps), int(tail_boost), int(inflight), int(block),
-                                      float(electron_split), int(electron_chsteps)), self.h)
+                                      float(electron_split), int(electron_chsteps), int(drain_particles)), self.h)
 
     def profile_trace(self):
         """Per-cycle trace of the last profiled event-form run: array of rows
