@@ -412,11 +412,12 @@ __global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_split_step(DevData<floa
 
 // Electron/positron events of the queued charged particles: at most the
 // cycle's budget of tstep-loop iterations each, then the particle is
-// re-queued.  Four resident blocks of 256 threads per SM (64 registers,
-// a few spills) measured faster than three (80) or two (114): the step is
-// latency bound and more warps hide more of it.
+// re-queued.  The step is latency bound and more resident warps hide more
+// of it: eight blocks of 256 threads per SM (full occupancy, 32 registers
+// with spills to L1-cached local memory) measured 5 % faster than four
+// (64 registers) and 12 % faster than two (114 registers, no spills).
 template <bool DEFER>
-__global__ void __launch_bounds__(EV_MAX_BLOCK, 4) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
+__global__ void __launch_bounds__(EV_MAX_BLOCK, 8) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
                                                        double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
                                                        int *live, int nbmax, Queue qi) {
     transport_events<DEFER ? EV_ELECTRON_DEFER : EV_ELECTRON>(D, in, outP, outE, tallies, nvox, ctl, seedw, live,
@@ -459,7 +460,7 @@ struct DrainPart {
     uint32_t k0, k1, pos;
 };
 
-__global__ void __launch_bounds__(DRAIN_BLOCK) k_drain(DevData<float> D, Queue qP, Queue qE, double *tallies,
+__global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queue qP, Queue qE, double *tallies,
                                                         long nvox, Ctl *ctl, uint32_t seedw) {
     const int np = queue_size(qP), ne = queue_size(qE);
     const int n = np + ne;
