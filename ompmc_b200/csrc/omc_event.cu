@@ -777,14 +777,15 @@ static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, doubl
 }
 
 // Particles left in the queues at or below which the transport switches
-// from cycles to the drain (0: never).  By default half the drain kernel's
-// resident threads: the drain serialises each particle's whole remaining
-// cascade in one thread, so it pays only once the cycles are mostly idle
-// (measured on slab64: 40 k best of 5 k - 1 M particles, +11 %).
+// from cycles to the drain (0: never).  By default a quarter of the drain
+// kernel's resident threads: the drain serialises each particle's whole
+// remaining cascade in one thread, so it pays only once the cycles are
+// mostly idle (measured on slab64: ≈40 k best of 5 k - 1 M particles, for
+// 10^6- and 10^7-history runs alike).
 static long long drain_threshold(const omc_engine *e) {
     const EventState &S = *e->ev;
     if (e->d32.d.nsplit > 1 || e->opt.drain_particles < 0) return 0;
-    return e->opt.drain_particles > 0 ? e->opt.drain_particles : S.drain_lanes / 2;
+    return e->opt.drain_particles > 0 ? e->opt.drain_particles : S.drain_lanes / 4;
 }
 
 // The drain over the queues `iph`/`iph + 1` holding `left` particles.
