@@ -363,7 +363,8 @@ def main():
         # the same beam (untimed; results do not depend on them); shorter
         # runs over-weight the end of a run, where other settings win
         from ompmc_b200.autotune import tune_beam
-        cfg, rate, trials = tune_beam(eng, nhist=min(nstep, 3_000_000), spectrum=spec, collimator=COLLIMATOR)
+        cfg, rate, trials = tune_beam(eng, nhist=min(nstep, 3_000_000), repeats=3, spectrum=spec,
+                                      collimator=COLLIMATOR)
         tuned = dict(cfg, trials=len(trials), tune_hist_per_s=rate)
     for i in range(args.warmup):
         step(-1 - i)

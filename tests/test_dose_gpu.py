@@ -48,3 +48,57 @@ def test_dose_z_scores(fixture, mode, golden, engine_for, assets_root):
     frac = np.mean(np.abs(z) < 3)
     assert frac >= 0.99, f"{fixture} mode {mode}: |z|<3 in {frac:.4f}; mean z {z.mean():.3f}"
     assert abs(z.mean()) < 0.25, f"{fixture} mode {mode}: biased, mean z {z.mean():.3f}"
+
+
+# The event form's alternatives to its defaults stay pinned to the reference:
+# photons walked voxel by voxel (non-uniform grids use it), the reference's
+# per-step restart of the interaction distance, no drain kernel, and
+# interactions sampled in place.
+VARIANTS = {
+    "voxel_walk": dict(photon_woodcock=0),
+    "reference_restart": dict(electron_chsteps=0),
+    "no_drain_inplace": dict(drain_particles=-1, electron_interact_kernel=0),
+}
+
+
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
+def test_event_variants_match_reference(variant, golden, assets_root):
+    from ompmc_b200.engine import EVENT_FP32, Engine, Tables, load_spectrum
+    from tests.conftest import case_phantom
+    g = golden("dose_slab64")
+    eng = Engine(Tables.from_assets(CASES["slab64"]["media"], assets_root), case_phantom("slab64"),
+                 **VARIANTS[variant])
+    spec = load_spectrum(assets_root / "spectra" / "6mv.spectrum")
+    dose, unc, st = eng.run_beam(int(g["ncase"]), 50, seed=777, mode=EVENT_FP32, spectrum=spec,
+                                 collimator=CASES["slab64"]["collimator"])
+    eng.close()
+    assert st["flags"] == 0
+    d = dose.ravel()[g["idx"]]
+    u = unc.ravel()[g["idx"]]
+    sel = g["dose"] > 0.10 * g["dmax"]
+    z = (d - g["dose"])[sel] / np.sqrt((u * d) ** 2 + (g["unc"] * g["dose"]) ** 2)[sel]
+    assert np.mean(np.abs(z) < 3) >= 0.99, f"{variant}: |z|<3 in {np.mean(np.abs(z) < 3):.4f}"
+    assert abs(z.mean()) < 0.25, f"{variant}: mean z {z.mean():.3f}"
+
+
+def test_nonuniform_grid_event_matches_plain(assets_root):
+    """A grid with voxels of two sizes (the event form then walks photons
+    voxel by voxel): event and plain FP64 forms agree statistically."""
+    from ompmc_b200 import assets as A
+    from ompmc_b200.engine import EVENT_FP32, PLAIN_FP64, Engine, Tables, load_spectrum
+    ph = A.slab_phantom(48, 0.25)
+    zb = np.concatenate([np.arange(0, 6.0, 0.5), np.arange(6.0, 12.0 + 1e-9, 0.1666666)])[: 49]
+    zb = np.round(zb, 6)
+    ph = A.Phantom(ph.media, ph.xb, ph.yb, zb, ph.med, ph.rho, name="slab_nonuniform")
+    eng = Engine(Tables.from_assets(CASES["slab64"]["media"], assets_root), ph)
+    spec = load_spectrum(assets_root / "spectra" / "6mv.spectrum")
+    kw = dict(spectrum=spec, collimator=(-2.5, 2.5, -2.5, 2.5))
+    d1, u1, s1 = eng.run_beam(2_000_000, 20, seed=5, mode=EVENT_FP32, **kw)
+    d0, u0, s0 = eng.run_beam(1_000_000, 20, seed=6, mode=PLAIN_FP64, **kw)
+    eng.close()
+    assert s1["flags"] == 0 and s0["flags"] == 0
+    m = d0 > 0.10 * d0.max()
+    z = (d1 - d0)[m] / np.sqrt((u1 * d1) ** 2 + (u0 * d0) ** 2)[m]
+    assert m.sum() > 500
+    assert np.mean(np.abs(z) < 3) >= 0.99, np.mean(np.abs(z) < 3)
+    assert abs(z.mean()) < 0.25, z.mean()
