@@ -450,18 +450,23 @@ __global__ void __launch_bounds__(EV_MAX_BLOCK) k_electron_interact(DevData<floa
 // interaction without a budget (budgets do not change trajectories) and
 // interactions are sampled in place (the same draws as the interaction
 // kernel), so the dose is the one the cycles would have produced, up to
-// the summation order of the FP64 tallies.  Not used with photon
-// splitting.
+// the summation order of the FP64 tallies.  SPLIT: photons are split rays
+// (nsplit > 1) whose state (next sub-photon, survivor, offset) rides on the
+// stack with them, as in the photon queues.
 constexpr int DRAIN_STACK = 48;
 constexpr int DRAIN_BLOCK = 128;
 
 struct DrainPart {
     Part<float> p;
     uint32_t k0, k1, pos;
+    int sp;       // splitting state (-1: not yet split)
+    float sr;
 };
 
+template <bool SPLIT>
 __global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queue qP, Queue qE, double *tallies,
                                                         long nvox, Ctl *ctl, uint32_t seedw) {
+    constexpr int MAXOUT = SPLIT ? EV_MAXOUT_SPLIT : EV_MAXOUT;
     const int np = queue_size(qP), ne = queue_size(qE);
     const int n = np + ne;
     DrainPart st[DRAIN_STACK];
@@ -471,8 +476,11 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queu
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const Queue &q = t < np ? qP : qE;
         int tag = 0;
-        qload(q, queue_index(q, t < np ? t : t - np), st[0].p, tag, st[0].k0, st[0].k1, st[0].pos);
-        EvEnv<EV_MAXOUT> g;
+        const int qi = queue_index(q, t < np ? t : t - np);
+        qload(q, qi, st[0].p, tag, st[0].k0, st[0].k1, st[0].pos);
+        st[0].sp = (SPLIT && q.sp) ? q.sp[qi] : -1;
+        st[0].sr = (SPLIT && q.sr) ? q.sr[qi] : 0.f;
+        EvEnv<MAXOUT> g;
         g.tally = tallies + (long)(tag >> 2) * nvox;
         g.pend_ir = -1;
         g.pend_e = 0.0;
@@ -493,8 +501,12 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queu
             g.tleft = 1 << 30;
             g.ncross = g.ndep = 0;
             const int kind = p.iq == 0 ? 0 : 1;
-            bool alive = kind == 0 ? (D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p))
-                                   : electron_step<float, EvEnv<EV_MAXOUT>, false>(D, g, p) == E_ALIVE;
+            int sp = e.sp;
+            float sr = e.sr;
+            bool alive;
+            if (kind == 1) alive = electron_step<float, EvEnv<MAXOUT>, false>(D, g, p) == E_ALIVE;
+            else if (SPLIT) alive = split_event(D, g, p, sp, sr);
+            else alive = D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p);
             c_ev[kind]++;
             c_steps[kind] += g.work;
             c_cross[kind] += g.ncross;
@@ -507,6 +519,8 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queu
             if (alive) {
                 e.p = p;
                 e.pos = g.rng.position();
+                e.sp = sp;
+                e.sr = sr;
             } else {
                 top--;
             }
@@ -528,6 +542,8 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queu
                 st[top].k0 = (uint32_t)ck;
                 st[top].k1 = (uint32_t)(ck >> 32);
                 st[top].pos = 0;
+                st[top].sp = -1;
+                st[top].sr = 0.f;
             }
         }
         g.flush();
@@ -660,7 +676,7 @@ static void size_grids(omc_engine *e, EventState &S) {
     int bi = 0, bd = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_electron_interact, S.block, 0);
     S.grid_i = e->sm_count * std::max(1, bi);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_drain, DRAIN_BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_drain<false>, DRAIN_BLOCK, 0);
     S.drain_lanes = e->sm_count * std::max(1, bd) * DRAIN_BLOCK;
     S.lanes = S.grid_e * S.block;
 }
@@ -784,7 +800,7 @@ static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, doubl
 // 10^6- and 10^7-history runs alike).
 static long long drain_threshold(const omc_engine *e) {
     const EventState &S = *e->ev;
-    if (e->d32.d.nsplit > 1 || e->opt.drain_particles < 0) return 0;
+    if (e->opt.drain_particles < 0) return 0;
     return e->opt.drain_particles > 0 ? e->opt.drain_particles : S.drain_lanes / 4;
 }
 
@@ -793,8 +809,9 @@ static void launch_drain(omc_engine *e, int iph, long long left, double *tallies
     EventState &S = *e->ev;
     long long g = (left + DRAIN_BLOCK - 1) / DRAIN_BLOCK;
     g = std::max(1LL, std::min(g, (long long)S.drain_lanes / DRAIN_BLOCK * 4));
-    k_drain<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[iph + 1], tallies, e->ph.nvox(), S.ctl_d,
-                                                   (uint32_t)(seed >> 32));
+    auto kd = e->d32.d.nsplit > 1 ? k_drain<true> : k_drain<false>;
+    kd<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[iph + 1], tallies, e->ph.nvox(), S.ctl_d,
+                                              (uint32_t)(seed >> 32));
 }
 
 // Profiled transport: cycles launched one by one with events around each

@@ -27,7 +27,8 @@ CONFIGS = {
     # photon splitting: a split photon's state (sub-photon, survivor,
     # stratification offset) is carried from event to event
     "nsplit5": [dict(nsplit=5, electron_tsteps=1, tail_boost=1, electron_split=0.0), dict(nsplit=5),
-                dict(nsplit=5, block=128, inflight=1 << 18)],
+                dict(nsplit=5, block=128, inflight=1 << 18), dict(nsplit=5, drain_particles=-1),
+                dict(nsplit=5, drain_particles=1 << 22)],
 }
 
 
