@@ -60,7 +60,8 @@ def tune_beam(eng, nhist=200_000, space=None, repeats=2, rounds=2, log=None, **r
     `nhist` histories of the beam given by `run_kw` (spectrum, collimator,
     ...).  Returns (best config, histories/s, list of (config, rate))."""
     space = dict(space or SPACE)
-    cur = dict(DEFAULT)
+    # start from DEFAULT, each parameter moved into the searched values
+    cur = {k: (v if k not in space or v in space[k] else space[k][0]) for k, v in DEFAULT.items()}
     seen = {}
 
     def measure(cfg):
