@@ -1,6 +1,7 @@
 """Autotuner (ompmc_b200.autotune): the search returns a setting from its
 space, leaves the engine at it, and the tuned engine's dose equals the
-default engine's up to the FP64 summation order."""
+default engine's (at the same electron_chsteps) up to the FP64 summation
+order."""
 import numpy as np
 import pytest
 
@@ -27,7 +28,9 @@ def test_tune_beam_small_space(engine_for, assets_root):
     assert rate > 0 and len(trials) >= 5
     d1, _, _ = eng.run_beam(100_000, 10, seed=5, mode=EVENT_FP32, spectrum=spec, collimator=coll)
     eng.close()
-    ref = Engine(t, ph)
+    # electron_chsteps changes which random numbers a trajectory draws (not
+    # the distribution it samples): the reference uses the tuned value
+    ref = Engine(t, ph, electron_chsteps=cfg["electron_chsteps"])
     d0, _, _ = ref.run_beam(100_000, 10, seed=5, mode=EVENT_FP32, spectrum=spec, collimator=coll)
     ref.close()
     m = d0 > 0
