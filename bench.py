@@ -173,20 +173,23 @@ def reference_rate(root, ph, spec_path, ncase, cores):
 GANTRY = [0.0, 51.0, 103.0, 154.0, 206.0, 257.0, 309.0]
 
 
-def bench_serving(device, nbeamlets, load=0.7, seed=7, plain_sample=12):
+def bench_serving(device, nbeamlets, load=0.7, seed=7, plain_sample=12, params=None):
     """beamlet dose-influence requests on the 128x128x96
     x 0.3 cm CT-like phantom, 7 coplanar beams, 0.5x0.5 cm2 bixels at the
     isocentre (SAD 100 cm), histories per beamlet log-uniform in
     [2e4, 2e5], Poisson arrivals offered at `load` x measured capacity.
     Returns latency percentiles and throughput of the served event form and
     the plain FP64 form on a sample of the same beamlets (run one after the
-    other, as the reference does)."""
+    other, as the reference does).  `params`: event-form parameters
+    (Engine.event_params keywords) set before the server is created."""
     from ompmc_b200 import assets as A
     from ompmc_b200.engine import PLAIN_FP64, Engine, Server, Tables, bixel_grid, load_spectrum
     root = A.require_assets()
     ph = A.ct_phantom(128, 128, 96, 0.3, seed=1234)
     spec = load_spectrum(root / "spectra" / "6mv.spectrum")
     eng = Engine(Tables.from_assets(A.CT_MEDIA, root), ph, device=device)
+    if params:
+        eng.event_params(**params)
     bl = bixel_grid(ph, GANTRY, bixel=0.5, field=(8.5, 8.5))        # 7 x 17 x 17 = 2023 bixels
     bl["spectrum"] = spec
     rng = np.random.default_rng(seed)

@@ -798,20 +798,21 @@ static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, doubl
 // remaining cascade in one thread, so it pays only once the cycles are
 // mostly idle (measured on slab64: ≈40 k best of 5 k - 1 M particles, for
 // 10^6- and 10^7-history runs alike).
-static long long drain_threshold(const omc_engine *e) {
+long long drain_threshold(const omc_engine *e) {
     const EventState &S = *e->ev;
     if (e->opt.drain_particles < 0) return 0;
     return e->opt.drain_particles > 0 ? e->opt.drain_particles : S.drain_lanes / 4;
 }
 
-// The drain over the queues `iph`/`iph + 1` holding `left` particles.
-static void launch_drain(omc_engine *e, int iph, long long left, double *tallies, uint64_t seed) {
+// The drain over the queues `iph`/`iph + 1` holding `left` particles, on
+// the streams of the cycles that filled them (seed word `seedw`).
+static void launch_drain(omc_engine *e, int iph, long long left, double *tallies, uint32_t seedw) {
     EventState &S = *e->ev;
     long long g = (left + DRAIN_BLOCK - 1) / DRAIN_BLOCK;
     g = std::max(1LL, std::min(g, (long long)S.drain_lanes / DRAIN_BLOCK * 4));
     auto kd = e->d32.d.nsplit > 1 ? k_drain<true> : k_drain<false>;
     kd<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[iph + 1], tallies, e->ph.nvox(), S.ctl_d,
-                                              (uint32_t)(seed >> 32));
+                                              seedw);
 }
 
 // Profiled transport: cycles launched one by one with events around each
@@ -853,7 +854,7 @@ static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallie
         long long dthr = drain_threshold(e);
         if (dthr > 0 && h.hist_next >= h.hist_total && cnt_in[0] + cnt_in[1] <= dthr) {
             cudaEventRecord(ev[0], e->stream);
-            launch_drain(e, oph, (long long)cnt_in[0] + cnt_in[1], tallies, seed);
+            launch_drain(e, oph, (long long)cnt_in[0] + cnt_in[1], tallies, (uint32_t)(seed >> 32));
             cudaEventRecord(ev[1], e->stream);
             if ((rc = cuda_check(e, cudaEventSynchronize(ev[1]), "drain"))) break;
             float td = 0;
@@ -968,7 +969,7 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
             long long left = (long long)std::min(h.cnt[0] + h.cnt_hi[0], S.cap) +
                              std::min(h.cnt[1] + h.cnt_hi[1], S.cap);
             if (left <= dthr) {
-                launch_drain(e, 0, left, tal.as<double>(), seed);
+                launch_drain(e, 0, left, tal.as<double>(), (uint32_t)(seed >> 32));
                 drains = 1;
                 if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "drain"))) break;
                 cudaMemcpy(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
@@ -1074,7 +1075,7 @@ void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, in
     EventState &S = *e->ev;
     int iph = in == 0 ? 0 : 2, iel = iph + 1;
     int oph = in == 0 ? 2 : 0, oel = oph + 1;
-    uint32_t seedw = 0x5e7e5eedu;
+    const uint32_t seedw = SERVE_SEEDW;
     long nvox = e->ph.nvox();
     k_serve_plan<<<1, 1, 0, e->stream>>>(sd, S.ctl_d, iph, iel, plan_cfg(e, target));
     k_serve_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, sd, S.q[iph], S.q[iel], S.ctl_d, nbmax, seedw);
@@ -1085,6 +1086,17 @@ void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, in
     if (e->d32.d.defer_interact)
         k_electron_interact<<<S.grid_i, S.block, 0, e->stream>>>(e->d32.d, S.qi, S.q[oph], S.q[oel], tallies, nvox,
                                                                  S.ctl_d, seedw, sd->live, nbmax, S.qi);
+}
+
+// The drain in serving: the particles left in queues A (where a graph of
+// two cycles leaves them) run to the end on the serving streams; then the
+// queues are emptied and every request's live count is zero.
+void serve_drain(omc_engine *e, ServeDev *sd, long long left, double *tallies) {
+    EventState &S = *e->ev;
+    launch_drain(e, 0, left, tallies, SERVE_SEEDW);
+    cudaMemsetAsync(sd->live, 0, sizeof(sd->live), e->stream);
+    cudaMemsetAsync(S.ctl_d->cnt, 0, 2 * sizeof(int), e->stream);
+    cudaMemsetAsync(S.ctl_d->cnt_hi, 0, 2 * sizeof(int), e->stream);
 }
 
 }  // namespace omc

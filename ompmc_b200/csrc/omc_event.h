@@ -91,6 +91,7 @@ struct EventState {
 
 // ------------------------------------------------------------ serving
 constexpr int SERVE_MAX = 256;  // request slots resident on the device
+constexpr uint32_t SERVE_SEEDW = 0x5e7e5eedu;  // seed word of the serving streams
 
 // One admitted request: its histories are injected from `next` on; kind -1
 // marks a free slot.
@@ -122,6 +123,10 @@ int event_interact_queue(omc_engine *e);
 // One serving cycle with input buffers `in` (0 = A, 1 = B); tally slot of a
 // particle = request slot * nbmax + batch.
 void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
+void serve_drain(omc_engine *e, ServeDev *sd, long long left, double *tallies);
+// Particles left at or below which a run whose histories are all injected
+// switches from transport cycles to the drain kernel (0: never).
+long long drain_threshold(const omc_engine *e);
 PlanCfg plan_cfg(const omc_engine *e, long long target);
 int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, int block, double split_kinetic);
 

@@ -5,8 +5,11 @@
 // device slot: a ServeReq entry, a source descriptor and nbatch FP64 working
 // tallies.  Every transport cycle a planner kernel hands out injection room
 // first come first served; the transport kernels keep a live-particle count
-// per request.  A request is finished when all its histories are injected and
-// its live count is zero; the host then folds its batch tallies, finalises
+// per request.  When every admitted history is injected, nothing is pending
+// and few particles are left, the drain kernel runs them to the end in one
+// launch instead of the cycles' long tail.  A request is finished when all
+// its histories are injected and its live count is zero; the host then
+// folds its batch tallies, finalises
 // dose and uncertainty (matRad: variance of the mean), extracts the sparse
 // column (entries above rel_threshold * column maximum, rows ascending), frees
 // the slot and admits the next pending request.  The sequential beamlet loop
@@ -204,7 +207,11 @@ struct omc_server {
     std::map<const omc_beamlets *, std::unique_ptr<PlanBuf>> plans;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    long long cycles = 0;
+    long long cycles = 0, drains = 0;
+    // state after the last step: particles in the queues, and whether every
+    // running request had all its histories injected
+    long long left = 0;
+    bool injected = false;
     // finalise scratch (device): sum, sum2, dose, var | rows | vals | vars | seg counts/offsets | dmax | total
     double *f_sum = nullptr, *f_sum2 = nullptr, *f_dose = nullptr, *f_var = nullptr, *f_vals = nullptr,
            *f_vars = nullptr;
@@ -271,6 +278,7 @@ int admit(omc_server *s) {
         s->pending.pop_front();
         r.slot = slot;
         r.state = 1;
+        s->injected = false;
         s->slot_req[slot] = r.id;
         s->order.push_back(slot);
         ServeReq q{};
@@ -444,23 +452,36 @@ int omc_server_step(omc_server *s, int cycles, int *active) {
     int rc = admit(s);
     if (rc) return rc;
     if (!s->order.empty()) {
-        int graphs = std::max(1, cycles / 2);
-        for (int k = 0; k < graphs; k++) cudaGraphLaunch(s->exec, e->stream);
-        s->cycles += 2 * graphs;
+        const long long dthr = drain_threshold(e);
+        if (dthr > 0 && s->injected && s->pending.empty() && s->left > 0 && s->left <= dthr) {
+            serve_drain(e, s->sd, s->left, s->tallies.as<double>());
+            s->drains++;
+        } else {
+            int graphs = std::max(1, cycles / 2);
+            for (int k = 0; k < graphs; k++) cudaGraphLaunch(s->exec, e->stream);
+            s->cycles += 2 * graphs;
+        }
         // completion check: all injected and nothing left in the queues
         std::vector<ServeReq> rq(s->nslots);
         std::vector<int> live(s->nslots);
         unsigned flags = 0;
+        int qc[8];  // Ctl::cnt, Ctl::cnt_hi
         cudaMemcpyAsync(rq.data(), s->sd->req, sizeof(ServeReq) * s->nslots, cudaMemcpyDeviceToHost, e->stream);
         cudaMemcpyAsync(live.data(), s->sd->live, sizeof(int) * s->nslots, cudaMemcpyDeviceToHost, e->stream);
         cudaMemcpyAsync(&flags, &e->ev->ctl_d->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpyAsync(qc, e->ev->ctl_d->cnt, sizeof(qc), cudaMemcpyDeviceToHost, e->stream);
         if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "server step"))) return rc;
         if (flags & (ERR_QUEUE | ERR_NAN | ERR_STACK))
             return set_err(e, OMC_E_DEVICE, "device error flags " + std::to_string(flags) + " in serving");
+        // a graph ends with a B -> A cycle: the particles are in queues A
+        const long long cap = e->ev->cap;
+        s->left = std::min<long long>(qc[0] + qc[4], cap) + std::min<long long>(qc[1] + qc[5], cap);
+        s->injected = true;
         std::vector<int> keep;
         bool freed = false;
         for (int slot : s->order) {
             Request &r = *s->reqs[s->slot_req[slot]];
+            if (rq[slot].next < r.nhist) s->injected = false;
             if (rq[slot].next >= r.nhist && live[slot] == 0) {
                 if ((rc = finalize_request(s, r))) return rc;
                 r.state = 2;
@@ -571,7 +592,7 @@ int omc_run_beamlets(omc_engine *e, const omc_beamlets *b, int64_t nhist, int nb
             cvar[i] = std::move(r.var);
             histories += r.nhist;
         }
-        launches = (double)s->cycles * (e->d32.d.defer_interact ? 5 : 4);
+        launches = (double)s->cycles * (e->d32.d.defer_interact ? 5 : 4) + (double)s->drains;
     } else if (mode == OMC_PLAIN_FP64) {
         PlanBuf pb;
         if ((rc = upload_plan<double>(e, b, pb.f64, pb.s64))) return rc;
