@@ -3,6 +3,9 @@
 * isolation: a request's result is the same alone and in a mix of other
   requests admitted at different times (same request seed; only the FP64
   summation order of the tally atomics may differ, rtol 1e-9);
+* the drain (the last particles run to the end in one launch once every
+  admitted history is injected) changes no result: the same request with
+  the drain off gives the same column;
 * admission by memory: with a budget for two requests, eight requests all
   finish, first come first served, with results identical to an unbounded
   server;
@@ -57,6 +60,28 @@ def test_result_same_alone_and_in_mix(engine_for, assets_root):
     np.testing.assert_allclose(b[1], a[1], rtol=1e-9)
     np.testing.assert_allclose(b[2], a[2], rtol=1e-6, atol=1e-40)
     assert len(a[0]) > 100
+
+
+def test_drain_changes_no_result(engine_for, assets_root):
+    from ompmc_b200.engine import Server, load_spectrum
+    eng = engine_for("ctsmall")
+    bl = bixels(engine_for)
+    bl["spectrum"] = load_spectrum(assets_root / "spectra" / "6mv.spectrum")
+    out = []
+    try:
+        for drain in (0, -1):                     # default threshold, then off
+            eng.event_params(drain_particles=drain)
+            srv = Server(eng, seed=5)
+            bs = srv.beamlet_set(bl)
+            out.append(run_all(srv, {"x": srv.submit_beamlet(bs, 6, 40000, 10, 1e-4, seed=4242)})["x"])
+            srv.close()
+    finally:
+        eng.event_params(drain_particles=0)
+    a, b = out
+    assert len(a[0]) > 100
+    assert np.array_equal(a[0], b[0])
+    np.testing.assert_allclose(b[1], a[1], rtol=1e-9)
+    np.testing.assert_allclose(b[2], a[2], rtol=1e-6, atol=1e-40)
 
 
 def test_admission_by_memory_budget(engine_for, assets_root):
