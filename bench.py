@@ -318,9 +318,18 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch parameters)")
     ap.add_argument("--cycle-trace", action="store_true",
                     help="print the per-cycle trace (queue sizes, kernel ms) of the first warm-up step and exit")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="run only the serving workload and print its JSON object")
+    ap.add_argument("--serving-params", default=None,
+                    help="event-form parameters of the serving engine, as JSON (Engine.event_params keywords)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    serving_params = json.loads(args.serving_params) if args.serving_params else None
+    if args.serving_only:
+        print(json.dumps({"serving": bench_serving(int(os.environ.get("LOCAL_RANK", "0")), args.serving_requests,
+                                                   params=serving_params), "params": serving_params}))
+        return 0
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -475,7 +484,7 @@ def main():
             else:
                 extras["cpu_baseline"] = None
         if args.serving_requests > 0 and world == 1:
-            extras["serving"] = bench_serving(local, args.serving_requests)
+            extras["serving"] = bench_serving(local, args.serving_requests, params=serving_params)
 
     if rank == 0:
         out = {
