@@ -266,8 +266,10 @@ int omc_server_destroy(omc_server *s);
 int omc_server_submit_beamlet(omc_server *s, const omc_beamlets *b, int ibixel, int64_t nhist, int nbatch,
                               double rel_threshold, uint64_t seed);
 int omc_server_submit_beam(omc_server *s, const omc_beam *b, int64_t nhist, int nbatch, uint64_t seed);
-/* Advances the device by up to `cycles` transport cycles; *active receives
- * the requests still running. */
+/* Advances the device by up to `cycles` transport cycles, or, when nothing
+ * is pending, every running request is fully injected and at most the
+ * engine's drain_particles are left, by one drain launch that runs them to
+ * the end; *active receives the requests still running. */
 int omc_server_step(omc_server *s, int cycles, int *active);
 /* Status of a request: OMC_OK when finished, OMC_E_NOTREADY while running. */
 int omc_server_poll(omc_server *s, int id, double *latency_ms);
