@@ -198,14 +198,20 @@ def bench_serving(device, nbeamlets, load=0.7, seed=7, plain_sample=12, params=N
     nh = np.exp(rng.uniform(np.log(2e4), np.log(2e5), size=len(pick))).astype(np.int64) // 10 * 10
     srv = Server(eng, seed=seed)
     bs = srv.beamlet_set(bl)
-    # capacity probe: 16 requests back to back
-    t0 = time.perf_counter()
-    ids = [srv.submit_beamlet(bs, int(pick[i % len(pick)]), 50000, 10, 1e-4) for i in range(16)]
-    while srv.step(8) > 0:
-        pass
-    cap_hps = 16 * 50000 / (time.perf_counter() - t0)
-    for r in ids:
-        srv.release(r)
+    # capacity probe: 16 requests back to back, after one untimed warm-up
+    # burst (the first launches of a process load the kernels); the median
+    # of three bursts
+    caps = []
+    for rep in range(4):
+        t0 = time.perf_counter()
+        ids = [srv.submit_beamlet(bs, int(pick[(i + 16 * rep) % len(pick)]), 50000, 10, 1e-4) for i in range(16)]
+        while srv.step(8) > 0:
+            pass
+        if rep > 0:
+            caps.append(16 * 50000 / (time.perf_counter() - t0))
+        for r in ids:
+            srv.release(r)
+    cap_hps = float(np.median(caps))
     rate = load * cap_hps / float(nh.mean())                            # requests per second
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(pick)))
     sub = {}
