@@ -327,7 +327,8 @@ def main():
     ap.add_argument("--serving-only", action="store_true",
                     help="run only the serving workload and print its JSON object")
     ap.add_argument("--serving-params", default=None,
-                    help="event-form parameters of the serving engine, as JSON (Engine.event_params keywords)")
+                    help="event-form parameters of the serving engine (and of the --cycle-trace run), as JSON "
+                         "(Engine.event_params keywords)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -368,11 +369,27 @@ def main():
         # same seed as the first warm-up step: the queue sizes per cycle are
         # those of the launches a profiler sees first
         te = Engine(tables, ph, ecut=0.7, pcut=0.01, device=local, profile=True)
+        if serving_params:
+            te.event_params(**serving_params)
+        # untimed small run first: the first launches of a process load the kernels
+        te.run_beam(max(nstep // 10, NBATCH), NBATCH, seed=seed0 - 2, mode=EVENT_FP32, spectrum=spec,
+                    collimator=COLLIMATOR)
         te.run_beam(nstep, NBATCH, seed=seed0 - 1, mode=EVENT_FP32, spectrum=spec, collimator=COLLIMATOR)
         rows = te.profile_trace()
         te.close()
         cols = ["injected", "photons", "electrons", "source_ms", "photon_ms", "electron_ms"]
-        print(json.dumps({"seed": seed0 - 1, "histories": nstep, "columns": cols, "cycles": rows.tolist()}))
+        # phases: cycles up to the last injection, cycles after it, the drain
+        # (a last row with no source or photon time)
+        ms = rows[:, 3:].sum(axis=1)
+        drained = len(rows) > 1 and rows[-1, 3] == 0 and rows[-1, 4] == 0
+        nc = len(rows) - (1 if drained else 0)
+        inj = np.nonzero(rows[:nc, 0] > 0)[0]
+        li = int(inj[-1]) if len(inj) else -1
+        phases = {"cycles": nc, "last_injection_cycle": li, "injection_ms": float(ms[:li + 1].sum()),
+                  "after_injection_ms": float(ms[li + 1:nc].sum()), "drain_ms": float(rows[-1, 5]) if drained else 0.0,
+                  "drain_particles": int(rows[-1, 1] + rows[-1, 2]) if drained else 0}
+        print(json.dumps({"seed": seed0 - 1, "histories": nstep, "params": serving_params, "phases": phases,
+                          "columns": cols, "cycles": rows.tolist()}))
         eng.close()
         return 0
     tuned = None
