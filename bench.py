@@ -253,6 +253,37 @@ def bench_serving(device, nbeamlets, load=0.7, seed=7, plain_sample=12, params=N
             "speedup_served_vs_plain": served / plain}
 
 
+def bench_served_beams(eng, spec, nhist, nreq):
+    """The bench's dose runs as `nreq` beam requests submitted together to
+    the continuous-batching server on the same (tuned) engine: the requests
+    share the particle queues, so one request's last particles overlap the
+    next one's injection and only the last request pays the end-of-run
+    tail.  Wall-clock histories/s from submission to the last request's
+    dose and uncertainty in host memory, after one untimed request."""
+    from ompmc_b200.engine import Server
+    srv = Server(eng, seed=11)
+    try:
+        r = srv.submit_beam(max(nhist // 10, NBATCH), NBATCH, spectrum=spec, collimator=COLLIMATOR)
+        while srv.step(16) > 0:
+            pass
+        srv.release(r)
+        t0 = time.perf_counter()
+        ids = [srv.submit_beam(nhist, NBATCH, spectrum=spec, collimator=COLLIMATOR) for _ in range(nreq)]
+        while srv.step(16) > 0:
+            pass
+        wall = time.perf_counter() - t0
+        lat = [srv.poll(i) for i in ids]
+        dose, unc = srv.result_dense(ids[-1])
+        unc1 = mean_unc_above_half(dose.ravel(), unc.ravel())
+        for i in ids:
+            srv.release(i)
+    finally:
+        srv.close()
+    return {"value": nreq * nhist / wall, "unit": "histories/s", "requests": nreq, "histories_per_request": nhist,
+            "wall_s": wall, "first_done_ms": min(lat), "last_done_ms": max(lat),
+            "mean_rel_unc_gt50pct_dmax": unc1}
+
+
 def reduce_max(vals, dist, device):
     """Element-wise maximum over ranks (the job's time is its slowest rank)."""
     if dist is None:
@@ -508,6 +539,8 @@ def main():
                 extras["cpu_baseline"] = None
         if args.serving_requests > 0 and world == 1:
             extras["serving"] = bench_serving(local, args.serving_requests, params=serving_params)
+        if not args.no_extras and world == 1 and mode == EVENT_FP32:
+            extras["served_beams"] = bench_served_beams(eng, spec, nstep, args.steps)
 
     if rank == 0:
         out = {
