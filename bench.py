@@ -174,7 +174,7 @@ GANTRY = [0.0, 51.0, 103.0, 154.0, 206.0, 257.0, 309.0]
 
 
 def bench_serving(device, nbeamlets, load=0.7, seed=7, plain_sample=12, params=None):
-    """beamlet dose-influence requests on the 128x128x96
+    """The beamlet serving workload: dose-influence requests on the 128x128x96
     x 0.3 cm CT-like phantom, 7 coplanar beams, 0.5x0.5 cm2 bixels at the
     isocentre (SAD 100 cm), histories per beamlet log-uniform in
     [2e4, 2e5], Poisson arrivals offered at `load` x measured capacity.
