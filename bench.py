@@ -407,6 +407,7 @@ def main():
                     collimator=COLLIMATOR)
         te.run_beam(nstep, NBATCH, seed=seed0 - 1, mode=EVENT_FP32, spectrum=spec, collimator=COLLIMATOR)
         rows = te.profile_trace()
+        drain = te.profile_drain()
         te.close()
         cols = ["injected", "photons", "electrons", "source_ms", "photon_ms", "electron_ms"]
         # phases: cycles up to the last injection, cycles after it, the drain
@@ -418,7 +419,7 @@ def main():
         li = int(inj[-1]) if len(inj) else -1
         phases = {"cycles": nc, "last_injection_cycle": li, "injection_ms": float(ms[:li + 1].sum()),
                   "after_injection_ms": float(ms[li + 1:nc].sum()), "drain_ms": float(rows[-1, 5]) if drained else 0.0,
-                  "drain_particles": int(rows[-1, 1] + rows[-1, 2]) if drained else 0}
+                  "drain_particles": int(rows[-1, 1] + rows[-1, 2]) if drained else 0, "drain": drain}
         print(json.dumps({"seed": seed0 - 1, "histories": nstep, "params": serving_params, "phases": phases,
                           "columns": cols, "cycles": rows.tolist()}))
         eng.close()

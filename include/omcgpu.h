@@ -153,6 +153,14 @@ int omc_profile_last(const omc_engine *e, double *out, int n);
  * of that run (0 when none was profiled). */
 int omc_profile_trace(const omc_engine *e, double *out, int max_cycles);
 
+/* The drain of the last profiled event-form beam run (no reference
+ * counterpart; instrumentation of this engine's end-of-run kernel): out
+ * (n >= 5) = its device ms, the particles it started from, and the
+ * largest sub-history one of its threads ran: events, events of the
+ * particle it started from, transport steps.  Zeros when the run had no
+ * drain. */
+int omc_profile_drain(const omc_engine *e, double *out, int n);
+
 /* ------------------------------------------------------------ sources */
 /* Energy distribution: a spectrum inverse CDF (cdf1/cdf2 of length n,
  * omc_dosxyz.c:474-494) or a mono-energetic source (n = 0). */

@@ -606,6 +606,12 @@ int omc_profile_last(const omc_engine *e, double *out, int n) {
     return OMC_OK;
 }
 
+int omc_profile_drain(const omc_engine *e, double *out, int n) {
+    if (!e || !out || n < 5) return global_err(OMC_E_ARG, "omc_profile_drain: bad argument");
+    for (int i = 0; i < 5; i++) out[i] = e->ev ? e->ev->drain_stats[i] : 0.0;
+    return OMC_OK;
+}
+
 int omc_profile_trace(const omc_engine *e, double *out, int max_cycles) {
     if (!e || (max_cycles > 0 && !out)) return global_err(OMC_E_ARG, "omc_profile_trace: bad argument");
     if (!e->ev) return 0;

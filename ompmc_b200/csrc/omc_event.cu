@@ -463,7 +463,8 @@ struct DrainPart {
     float sr;
 };
 
-template <bool SPLIT>
+// STATS (profiled runs): record the largest sub-history a thread ran.
+template <bool SPLIT, bool STATS = false>
 __global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queue qP, Queue qE, double *tallies,
                                                         long nvox, Ctl *ctl, uint32_t seedw) {
     constexpr int MAXOUT = SPLIT ? EV_MAXOUT_SPLIT : EV_MAXOUT;
@@ -487,7 +488,13 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queu
         g.flags = 0;
         g.natom = 0;
         int top = 0;
+        // this sub-history: events, events of its first particle, steps
+        int x_ev = 0, x_chain = 0, x_steps = 0;
+        bool first_alive = true;
         for (int guard = 0; top >= 0; guard++) {
+            const bool first = first_alive && top == 0;
+            x_ev++;
+            x_chain += first;
             if (guard > (1 << 22)) {
                 g.flags |= ERR_LOOP;
                 break;
@@ -508,6 +515,7 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queu
             else if (SPLIT) alive = split_event(D, g, p, sp, sr);
             else alive = D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p);
             c_ev[kind]++;
+            x_steps += g.work;
             c_steps[kind] += g.work;
             c_cross[kind] += g.ncross;
             c_dep[kind] += g.ndep;
@@ -523,6 +531,7 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queu
                 e.sr = sr;
             } else {
                 top--;
+                first_alive = first_alive && !first;
             }
             for (int k = 0; k < g.nout; k++) {
                 const Part<float> &s2 = g.out[k];
@@ -547,6 +556,11 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queu
             }
         }
         g.flush();
+        if (STATS) {
+            atomicMax(&ctl->drain_max_events, x_ev);
+            atomicMax(&ctl->drain_max_chain, x_chain);
+            atomicMax(&ctl->drain_max_steps, x_steps);
+        }
         c_atom[1] += g.natom;     // tally atomics of the whole sub-history
         flags |= g.flags;
     }
@@ -805,12 +819,15 @@ long long drain_threshold(const omc_engine *e) {
 }
 
 // The drain over the queues `iph`/`iph + 1` holding `left` particles, on
-// the streams of the cycles that filled them (seed word `seedw`).
-static void launch_drain(omc_engine *e, int iph, long long left, double *tallies, uint32_t seedw) {
+// the streams of the cycles that filled them (seed word `seedw`); `stats`
+// records its largest sub-history.
+static void launch_drain(omc_engine *e, int iph, long long left, double *tallies, uint32_t seedw,
+                         bool stats = false) {
     EventState &S = *e->ev;
     long long g = (left + DRAIN_BLOCK - 1) / DRAIN_BLOCK;
     g = std::max(1LL, std::min(g, (long long)S.drain_lanes / DRAIN_BLOCK * 4));
-    auto kd = e->d32.d.nsplit > 1 ? k_drain<true> : k_drain<false>;
+    auto kd = e->d32.d.nsplit > 1 ? (stats ? k_drain<true, true> : k_drain<true, false>)
+                                  : (stats ? k_drain<false, true> : k_drain<false, false>);
     kd<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[iph + 1], tallies, e->ph.nvox(), S.ctl_d,
                                               seedw);
 }
@@ -823,6 +840,7 @@ static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallie
     EventState &S = *e->ev;
     for (auto &p : S.prof) p = KernelProfile();
     S.trace.clear();
+    for (double &v : S.drain_stats) v = 0;
     cudaEvent_t ev[5];
     for (auto &x : ev) cudaEventCreate(&x);
     int rc = OMC_OK;
@@ -854,7 +872,7 @@ static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallie
         long long dthr = drain_threshold(e);
         if (dthr > 0 && h.hist_next >= h.hist_total && cnt_in[0] + cnt_in[1] <= dthr) {
             cudaEventRecord(ev[0], e->stream);
-            launch_drain(e, oph, (long long)cnt_in[0] + cnt_in[1], tallies, (uint32_t)(seed >> 32));
+            launch_drain(e, oph, (long long)cnt_in[0] + cnt_in[1], tallies, (uint32_t)(seed >> 32), true);
             cudaEventRecord(ev[1], e->stream);
             if ((rc = cuda_check(e, cudaEventSynchronize(ev[1]), "drain"))) break;
             float td = 0;
@@ -864,6 +882,9 @@ static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallie
             S.prof[2].seconds += td * 1e-3;
             S.prof[2].launches += 1;
             cudaMemcpy(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
+            double ds[5] = {(double)td, (double)cnt_in[0] + cnt_in[1], (double)h.drain_max_events,
+                            (double)h.drain_max_chain, (double)h.drain_max_steps};
+            std::copy(ds, ds + 5, S.drain_stats);
             break;
         }
         if (cycles > 200000) {

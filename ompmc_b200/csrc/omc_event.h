@@ -45,6 +45,9 @@ struct Ctl {
     int pad3;
     // counters per transport kernel (0 photon, 1 electron)
     unsigned long long st_events[2], st_steps[2], st_cross[2], st_dep[2], st_atom[2];
+    // drain: the largest sub-history one thread ran (events, events of the
+    // particle it started from, transport steps)
+    int drain_max_events, drain_max_chain, drain_max_steps, drain_pad;
 };
 
 // Per-kernel profile of the last run made with options.profile = 1.
@@ -87,6 +90,9 @@ struct EventState {
     // profiled runs: per cycle {histories injected, photons in, electrons in,
     // source ms, photon ms, electron ms}
     std::vector<double> trace;
+    // profiled runs: the drain's ms, particles, and largest sub-history
+    // (events, events of its first particle, transport steps); zeros if none
+    double drain_stats[5] = {0, 0, 0, 0, 0};
 };
 
 // ------------------------------------------------------------ serving

@@ -103,6 +103,7 @@ def lib():
         "omc_dosxyz_run": ([C.c_char_p, C.c_char_p, C.c_int, C.c_int], C.c_int),
         "omc_profile_last": ([C.c_void_p, _dp, C.c_int], C.c_int),
         "omc_profile_trace": ([C.c_void_p, _dp, C.c_int], C.c_int),
+        "omc_profile_drain": ([C.c_void_p, _dp, C.c_int], C.c_int),
         "omc_event_params": ([C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int, C.c_double, C.c_int, C.c_int64],
                              C.c_int),
         "omc_run_beam_noalloc": ([C.c_void_p, C.POINTER(_Beam), C.c_int64, C.c_int, C.c_uint64, _dp, _dp, _dp],
@@ -367,6 +368,15 @@ class Engine:
         electron_chsteps, -2 for drain_particles, keeps the current value)."""
         _check(lib().omc_event_params(self.h, int(electron_tsteps), int(tail_boost), int(inflight), int(block),
                                       float(electron_split), int(electron_chsteps), int(drain_particles)), self.h)
+
+    def profile_drain(self):
+        """The drain of the last profiled event-form run: device ms, the
+        particles it started from, and its largest thread sub-history
+        (events, events of its first particle, transport steps)."""
+        out = np.zeros(5)
+        _check(lib().omc_profile_drain(self.h, _p(out, _dp), 5), self.h)
+        return {"ms": out[0], "particles": int(out[1]), "max_events": int(out[2]), "max_chain_events": int(out[3]),
+                "max_steps": int(out[4])}
 
     def profile_trace(self):
         """Per-cycle trace of the last profiled event-form run: array of rows
