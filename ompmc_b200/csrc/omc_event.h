@@ -93,6 +93,15 @@ struct EventState {
     // profiled runs: the drain's ms, particles, and largest sub-history
     // (events, events of its first particle, transport steps); zeros if none
     double drain_stats[5] = {0, 0, 0, 0, 0};
+    // second stream of the captured cycles: the photon kernel runs there,
+    // beside the electron kernels of its cycle (fork/join events)
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    ~EventState() {
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
+    }
 };
 
 // ------------------------------------------------------------ serving
