@@ -284,6 +284,22 @@ def bench_served_beams(eng, spec, nhist, nreq):
             "mean_rel_unc_gt50pct_dmax": unc1}
 
 
+def trace_phases(rows):
+    """Phases of a profiled run from its per-cycle trace (rows of injected,
+    photons, electrons, source ms, photon ms, electron ms): the cycles up to
+    the last injection, the cycles after it, and the drain (a last row with
+    no source or photon time)."""
+    rows = np.asarray(rows, dtype=np.float64).reshape(-1, 6)
+    ms = rows[:, 3:].sum(axis=1)
+    drained = len(rows) > 1 and rows[-1, 3] == 0 and rows[-1, 4] == 0
+    nc = len(rows) - (1 if drained else 0)
+    inj = np.nonzero(rows[:nc, 0] > 0)[0]
+    li = int(inj[-1]) if len(inj) else -1
+    return {"cycles": nc, "last_injection_cycle": li, "injection_ms": float(ms[:li + 1].sum()),
+            "after_injection_ms": float(ms[li + 1:nc].sum()), "drain_ms": float(rows[-1, 5]) if drained else 0.0,
+            "drain_particles": int(rows[-1, 1] + rows[-1, 2]) if drained else 0}
+
+
 def reduce_max(vals, dist, device):
     """Element-wise maximum over ranks (the job's time is its slowest rank)."""
     if dist is None:
@@ -410,16 +426,7 @@ def main():
         drain = te.profile_drain()
         te.close()
         cols = ["injected", "photons", "electrons", "source_ms", "photon_ms", "electron_ms"]
-        # phases: cycles up to the last injection, cycles after it, the drain
-        # (a last row with no source or photon time)
-        ms = rows[:, 3:].sum(axis=1)
-        drained = len(rows) > 1 and rows[-1, 3] == 0 and rows[-1, 4] == 0
-        nc = len(rows) - (1 if drained else 0)
-        inj = np.nonzero(rows[:nc, 0] > 0)[0]
-        li = int(inj[-1]) if len(inj) else -1
-        phases = {"cycles": nc, "last_injection_cycle": li, "injection_ms": float(ms[:li + 1].sum()),
-                  "after_injection_ms": float(ms[li + 1:nc].sum()), "drain_ms": float(rows[-1, 5]) if drained else 0.0,
-                  "drain_particles": int(rows[-1, 1] + rows[-1, 2]) if drained else 0, "drain": drain}
+        phases = dict(trace_phases(rows), drain=drain)
         print(json.dumps({"seed": seed0 - 1, "histories": nstep, "params": serving_params, "phases": phases,
                           "columns": cols, "cycles": rows.tolist()}))
         eng.close()
