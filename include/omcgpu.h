@@ -115,7 +115,7 @@ typedef struct {
                              at most this many particles are left, they are
                              run to the end of their sub-histories in one
                              launch instead of further cycles (0 = default,
-                             a quarter of the drain kernel's resident threads;
+                             half of the drain kernel's resident threads;
                              -1 = never);
                              results do not depend on it */
 } omc_options;

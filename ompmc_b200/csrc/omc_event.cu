@@ -454,6 +454,10 @@ __global__ void __launch_bounds__(EV_MAX_BLOCK) k_electron_interact(DevData<floa
 // (nsplit > 1) whose state (next sub-photon, survivor, offset) rides on the
 // stack with them, as in the photon queues.
 constexpr int DRAIN_STACK = 48;
+// 4 resident blocks of 128 per SM: up to 128 registers and no spills.  The
+// drain's length is the latency of its longest sub-history in one thread,
+// which spilled registers lengthen; it never needs more lanes than
+// particles (1.2 % faster on slab64 than 8 blocks at 64 registers).
 constexpr int DRAIN_BLOCK = 128;
 
 struct DrainPart {
@@ -465,7 +469,7 @@ struct DrainPart {
 
 // STATS (profiled runs): record the largest sub-history a thread ran.
 template <bool SPLIT, bool STATS = false>
-__global__ void __launch_bounds__(DRAIN_BLOCK, 8) k_drain(DevData<float> D, Queue qP, Queue qE, double *tallies,
+__global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<float> D, Queue qP, Queue qE, double *tallies,
                                                         long nvox, Ctl *ctl, uint32_t seedw) {
     constexpr int MAXOUT = SPLIT ? EV_MAXOUT_SPLIT : EV_MAXOUT;
     const int np = queue_size(qP), ne = queue_size(qE);
@@ -842,15 +846,15 @@ static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, doubl
 }
 
 // Particles left in the queues at or below which the transport switches
-// from cycles to the drain (0: never).  By default a quarter of the drain
-// kernel's resident threads: the drain serialises each particle's whole
-// remaining cascade in one thread, so it pays only once the cycles are
-// mostly idle (measured on slab64: ≈40 k best of 5 k - 1 M particles, for
-// 10^6- and 10^7-history runs alike).
+// from cycles to the drain (0: never).  By default half of the drain
+// kernel's resident threads (≈38 k): the drain serialises each particle's
+// whole remaining cascade in one thread, so it pays only once the cycles
+// are mostly idle (measured on slab64: ≈40 k best of 5 k - 1 M particles,
+// for 10^6- and 10^7-history runs alike).
 long long drain_threshold(const omc_engine *e) {
     const EventState &S = *e->ev;
     if (e->opt.drain_particles < 0) return 0;
-    return e->opt.drain_particles > 0 ? e->opt.drain_particles : S.drain_lanes / 4;
+    return e->opt.drain_particles > 0 ? e->opt.drain_particles : S.drain_lanes / 2;
 }
 
 // The drain over the queues `iph`/`iph + 1` holding `left` particles, on
