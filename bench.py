@@ -1,20 +1,39 @@
-"""Benchmark: histories/s of the event-based FP32-transport / FP64-tally form
-on the heterogeneous slab workload (64^3 voxels of 0.25 cm: water 0-3 cm,
-lung 3-8 cm, bone 8-10 cm, water; 5x5 cm^2 field of the 6 MV-like spectrum,
-10^7 histories per dose run), one JSON line on stdout.
+"""Benchmark: the served beamlet dose-influence load on one B200, one JSON
+line on stdout.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload beamlets|slab64]
 
-A step is one complete dose run of 10^7 histories in 10 batches through
-omc_run_beam (dose + batch uncertainty out).  `value` is device time of the
-transport (CUDA events on the engine's stream, tables/phantom resident);
-`e2e` times the same calls from the host with the spectrum upload and the
-dose/uncertainty download inside.  Under torchrun every rank runs its own
+Workload (default, `beamlets`): 2023 beamlet requests, the dose-influence
+columns of a 7-beam coplanar plan (gantry 0, 51, 103, 154, 206, 257, 309
+degrees; 17 x 17 bixels of 0.5 cm at the isocentre, SAD 100 cm) on the seeded
+128x128x96 x 0.3 cm CT-like phantom, the 6 MV-like spectrum, histories per
+request log-uniform in [2e4, 2e5] (1.58e8 in all), 10 batches, sparse columns
+thresholded at 1e-4 of their maximum with the variance of the mean beside
+them.  A step is one pass of the whole load through the continuous-batching
+server (omc_server_*): requests arrive as a Poisson process (default
+4000/s, above what one GPU serves, so the server works through a backlog
+with every slot busy) and are admitted as slots and device memory free up;
+each finished column is copied into host memory as it is reported.
+`value` is the load's histories over the device time of the passes (CUDA
+events on the server's stream); `e2e` is the same over host wall-clock
+time, from the first submission to the last column in host memory.
+p50_ms/p99_ms are per-beamlet latencies (arrival to column in host memory)
+of one more pass at `--latency-load` of the measured throughput; the
+saturated passes' latencies are reported beside them.  `unc` gives the mean
+relative uncertainty of each column above 50 % of its maximum and the
+seconds to 1 % it implies.
+
+`--impl reference` runs ompMC's own matRad D_ij entry (omc_matrad.c,
+unmodified, built with OpenMP into oracle/_ref) on all host cores, one call
+per beamlet of a different sample of the same load each step, timing each
+call's beamlet loop.
+
+`--workload slab64` keeps the single-beam dose run: 10^7 histories of a 5x5
+cm^2 6 MV-like beam on the 64^3 x 0.25 cm water/lung/bone slab phantom
+through omc_run_beam per step.  Under torchrun every rank runs its own
 histories on its own GPU (weak scaling, no collective on the data path); the
 reported time is the maximum over ranks.
-
-`--impl reference` times ompMC's own OpenMP CLI (built from its sources into
-oracle/_ref) on this host's cores on a bounded sample of the same workload.
 """
 from __future__ import annotations
 
@@ -34,7 +53,11 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 METRIC = "histories/s at 1% dose unc. (served vs plain GPU vs CPU); p50/p99 beamlet ms"
-WORKLOAD = "slab64: 64^3 x 0.25 cm water/lung(0.26)/bone(1.85)/water, 5x5 cm2 6MV-like, 1e7 histories in 10 batches per step"
+WORKLOAD = ("beamlets: 2023 beamlet requests (7 coplanar beams x 17x17 bixels of 0.5 cm) on the 128x128x96 x 0.3 cm "
+            "CT-like phantom, 6MV-like, log-uniform 2e4-2e5 histories, 10 batches, sparse columns at 1e-4, Poisson "
+            "arrivals, served")
+SLAB_WORKLOAD = ("slab64: 64^3 x 0.25 cm water/lung(0.26)/bone(1.85)/water, 5x5 cm2 6MV-like, 1e7 histories in 10 "
+                 "batches per step")
 HIST_PER_STEP = 10_000_000
 NBATCH = 10
 COLLIMATOR = (-2.5, 2.5, -2.5, 2.5)
@@ -326,6 +349,8 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if getattr(args, "workload", "slab64") == "beamlets":
+        return run_reference_beamlets(args)
     from oracle import ref
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs an ompMC checkout at build time)"}))
@@ -347,7 +372,7 @@ def run_reference_arm(args):
         "warmup": args.warmup, "ms_per_step": 1000 * sum(secs) / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "sample_histories_per_step": sample, "parallelism": f"openmp{cores}"},
+        "config": {"workload": SLAB_WORKLOAD, "sample_histories_per_step": sample, "parallelism": f"openmp{cores}"},
         "cpu_baseline": {"value": value, "unit": "histories/s", "cores": cores, "kind": "reference",
                          "sample": f"{sample} histories x {args.steps} runs of the ompMC CLI (slab64)"},
         "e2e": {"value": value, "unit": "histories/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -356,29 +381,304 @@ def run_reference_arm(args):
     return 0
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="event", choices=["event", "plain"])
-    ap.add_argument("--hist-per-step", type=int, default=HIST_PER_STEP)
-    ap.add_argument("--ref-sample", type=int, default=10_000_000)
-    ap.add_argument("--no-extras", action="store_true", help="skip the CPU baseline and plain comparator")
-    ap.add_argument("--serving-requests", type=int, default=300,
-                    help="beamlet requests in the serving workload (0 skips it)")
-    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch parameters)")
-    ap.add_argument("--cycle-trace", action="store_true",
-                    help="print the per-cycle trace (queue sizes, kernel ms) of the first warm-up step and exit")
-    ap.add_argument("--serving-only", action="store_true",
-                    help="run only the serving workload and print its JSON object")
-    ap.add_argument("--serving-params", default=None,
-                    help="event-form parameters of the serving engine (and of the --cycle-trace run), as JSON "
-                         "(Engine.event_params keywords)")
-    args = ap.parse_args()
-    if args.impl == "reference":
-        return run_reference_arm(args)
+# --------------------------------------------------------------------------
+# The served beamlet load (the headline workload)
+# --------------------------------------------------------------------------
+def serve_load(srv, load, rate, seed, idx=None, cycles=8):
+    """One pass of the beamlet load through the server: the requests
+    `order[idx]` submitted at the arrival times of a Poisson process of
+    `rate` requests/s, each finished request's sparse column (rows, dose,
+    variance) copied into host memory as soon as the server reports it.
+    The beamlet set is uploaded at the first submission of the pass.
+    Returns histories, device ms of the pass (events on the server's
+    stream), wall seconds, latency from arrival and from submission (ms),
+    column uncertainty and histories per request, result bytes, and the
+    server's kernel launches during the pass."""
+    from ompmc_b200.workloads import LOAD_NBATCH, LOAD_REL, column_unc
+    order, nh, gaps = load["order"], load["nhist"], load["gaps"]
+    if idx is None:
+        idx = np.arange(len(order))
+    arrivals = np.cumsum(gaps[idx]) / rate
+    arrivals -= arrivals[0]
+    bl = dict(load["beamlets"], spectrum=load["spectrum"])
+    bs = srv.beamlet_set(bl)
+    st0 = srv.stats()
+    n = len(idx)
+    sub, out = {}, {}
+    k = 0
+    srv.timer_start()
+    t0 = time.perf_counter()
+    for guard in range(50_000_000):
+        now = time.perf_counter() - t0
+        while k < n and arrivals[k] <= now:
+            b = int(order[idx[k]])
+            rid = srv.submit_beamlet(bs, b, int(nh[idx[k]]), LOAD_NBATCH, LOAD_REL, seed=seed * 100003 + b + 1)
+            sub[rid] = (k, 1e3 * (now - arrivals[k]))
+            k += 1
+        active = srv.step(cycles)
+        for rid in srv.completed():
+            rows, vals, var = srv.result_sparse(rid)
+            out[rid] = (srv.poll(rid), column_unc(vals, var), len(rows))
+            srv.release(rid)
+        if active == 0:
+            if k == n:
+                break
+            time.sleep(max(0.0, min(0.002, arrivals[k] - (time.perf_counter() - t0))))
+    else:
+        raise RuntimeError("serving pass did not finish")
+    dev_ms = srv.timer_stop()
+    wall = time.perf_counter() - t0
+    st1 = srv.stats()
+    lat_sub = np.array([out[r][0] for r in sub])
+    lat = lat_sub + np.array([sub[r][1] for r in sub])
+    unc = np.array([out[r][1] for r in sub])
+    hist = np.array([nh[idx[sub[r][0]]] for r in sub], dtype=np.float64)
+    nnz = np.array([out[r][2] for r in sub], dtype=np.float64)
+    return dict(histories=float(hist.sum()), dev_ms=dev_ms, wall_s=wall, lat_ms=lat, lat_sub_ms=lat_sub, unc=unc,
+                nhist=hist, d2h_bytes=float(nnz.sum() * (4 + 8 + 8)), nnz=nnz,
+                launches=st1["launches"] - st0["launches"], cycles=st1["cycles"] - st0["cycles"])
+
+
+def unc_summary(unc, nhist, rate):
+    """Uncertainty of a set of beamlet columns: the mean relative
+    uncertainty above 50 % of each column's maximum, the per-history
+    relative variance (unc^2 * histories, which the histories needed for 1 %
+    divide by 1e-4), and the seconds to 1 % for one average beamlet at
+    `rate` histories/s."""
+    ok = np.isfinite(unc)
+    q = unc[ok] ** 2 * nhist[ok]
+    return {"mean_rel_unc_gt50pct_dmax": float(np.mean(unc[ok])), "rel_var_x_histories": float(np.mean(q)),
+            "histories_to_1pct_per_beamlet": float(np.mean(q) / 1e-4),
+            "seconds_to_1pct_per_beamlet": float(np.mean(q) / 1e-4 / rate), "beamlets": int(ok.sum())}
+
+
+def beamlet_engine(load, device, profile=False):
+    from ompmc_b200.engine import Engine, Tables, load_spectrum
+    from ompmc_b200 import assets as A
+    load["spectrum"] = load_spectrum(load["spectrum_file"])
+    eng = Engine(Tables.from_assets(load["media"], A.require_assets()), load["phantom"], ecut=0.7, pcut=0.01,
+                 device=device, profile=profile)
+    return eng
+
+
+def main_beamlets(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from ompmc_b200.engine import PLAIN_FP64, Server
+    from ompmc_b200.workloads import LOAD_NBATCH, LOAD_REL, beamlet_load
+    load = beamlet_load(args.load_seed)
+    eng = beamlet_engine(load, local)
+    srv = Server(eng, seed=rank_seed(rank))
+    seed0 = rank_seed(rank)
+    rate = args.arrival_rate
+    for i in range(args.warmup):
+        serve_load(srv, load, rate, seed0 - 1 - i)
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    passes = []
+    for i in range(args.steps):
+        passes.append(serve_load(srv, load, rate, seed0 + i))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    dev_s = sum(p["dev_ms"] for p in passes) * 1e-3
+    wall = sum(p["wall_s"] for p in passes)
+    dev_s, wall = reduce_max([dev_s, wall], dist, "cuda")
+    total = sum(p["histories"] for p in passes) * world
+    value = total / dev_s
+    e2e = total / wall
+    lat = np.concatenate([p["lat_ms"] for p in passes])
+    lat_sub = np.concatenate([p["lat_sub_ms"] for p in passes])
+    unc = np.concatenate([p["unc"] for p in passes])
+    nh = np.concatenate([p["nhist"] for p in passes])
+    launches = sum(p["launches"] for p in passes)
+    nreq = len(load["order"])
+    extras = {}
+    if rank == 0:
+        extras["unc"] = unc_summary(unc, nh, value)
+        extras["saturated"] = {"arrival_rate_req_per_s": rate, "p50_ms": float(np.percentile(lat, 50)),
+                               "p99_ms": float(np.percentile(lat, 99)),
+                               "p50_ms_from_submission": float(np.percentile(lat_sub, 50)),
+                               "p99_ms_from_submission": float(np.percentile(lat_sub, 99)),
+                               "mean_nnz_per_column": float(np.mean(np.concatenate([p["nnz"] for p in passes])))}
+        # latency under load: the same requests arriving at a fraction of
+        # the measured throughput (Poisson), one untimed pass
+        load_rate = args.latency_load * value / float(np.mean(load["nhist"]))
+        lp = serve_load(srv, load, load_rate, seed0 + 5000, cycles=4)
+        extras["latency_at_load"] = {"offered_load_frac": args.latency_load, "arrival_rate_req_per_s": load_rate,
+                                     "served_hist_per_s": lp["histories"] / lp["wall_s"],
+                                     "p50_ms": float(np.percentile(lp["lat_ms"], 50)),
+                                     "p99_ms": float(np.percentile(lp["lat_ms"], 99))}
+    srv.close()
+    if rank == 0 and not args.no_extras and world == 1:
+        extras.update(beamlet_extras(args, load, eng, value, local))
+    eng.close()
+    if rank == 0:
+        d2h = float(np.mean([p["d2h_bytes"] for p in passes]))
+        out = {
+            "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "p50_ms": extras.get("latency_at_load", {}).get("p50_ms"),
+            "p99_ms": extras.get("latency_at_load", {}).get("p99_ms"),
+            "config": {"workload": WORKLOAD, "requests_per_step": nreq,
+                       "histories_per_step": float(np.sum(load["nhist"])),
+                       "arrival_rate_req_per_s": rate, "nbatch": LOAD_NBATCH, "rel_threshold": LOAD_REL,
+                       "mode": "event FP32 transport / FP64 tallies, served (continuous batching)",
+                       "parallelism": f"replicas{world}", "load_seed": args.load_seed,
+                       "l2": "particle queues (0.87 GB) and per-request batch tallies (126 MB each, up to 254 "
+                             "requests resident) exceed L2; physics tables are L2-resident"},
+            "e2e": {"value": e2e, "unit": "histories/s",
+                    "h2d_bytes_per_step": int(4 * (3 * 7 + 9 * nreq + 2 * 1000) + 4 * nreq + 64 * nreq),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        out.update(extras)
+        print(json.dumps(out))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def beamlet_extras(args, load, eng, value, device):
+    """Roofline of the dominant kernel, the plain FP64 comparator and the CPU
+    reference on samples of the same load (rank 0, one GPU, untimed)."""
+    from ompmc_b200.engine import PLAIN_FP64, Server
+    extras = {}
+    peak, peak_kind = peaks()
+    # a profiled pass over part of the load: per-kernel device time and
+    # transport counters with the kernels launched one by one
+    pe = beamlet_engine(load, device, profile=True)
+    ps = Server(pe, seed=99)
+    sub = np.arange(min(args.profile_requests, len(load["order"])))
+    serve_load(ps, load, args.arrival_rate, 424242, idx=sub)
+    prof = pe.profile_last()
+    ps.close()
+    pe.close()
+    ek, pk = prof["electron"], prof["photon"]
+    lookups = 10 * ek["steps"] + 3 * ek["particles"]
+    alg_bytes = 8 * ek["cross"] + 16 * ek["dep"] + 8 * lookups
+    achieved = alg_bytes / ek["seconds"] / 1e9
+    tpe = ncu_traffic_per_event()
+    per_launch_events = ek["particles"] / max(1, ek["launches"])
+    total_s = sum(x["seconds"] for x in prof.values())
+    extras["roofline"] = {
+        "bound": "hbm", "kernel": "k_electron_step + k_electron_interact (+ k_drain)", "achieved": achieved,
+        "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+        "traffic": (tpe * per_launch_events) if tpe else None,
+        "algorithmic_bytes_per_launch": alg_bytes / max(1, ek["launches"]),
+        "state_bytes_per_launch": 104 * per_launch_events,
+        "avg_launch_ms": 1000 * ek["seconds"] / max(1, ek["launches"]),
+        "kernel_seconds": {k: v["seconds"] for k, v in prof.items()},
+        "kernel_share": {k: v["seconds"] / max(1e-12, total_s) for k, v in prof.items()},
+        "sample": f"profiled pass over {len(sub)} requests of the load",
+    }
+    hist = float(np.sum(load["nhist"][sub]))
+    extras["per_history"] = {k: (ek[k] + pk[k]) / hist for k in ("particles", "steps", "cross", "dep", "atom")}
+    # plain FP64 history-based form on a sample of the same beamlets, one
+    # after the other (omc_run_beamlets)
+    m = args.plain_sample
+    pick = load["order"][:m]
+    bl = load["beamlets"]
+    sample = dict(src=bl["src"], corner=bl["corner"][pick], side1=bl["side1"][pick], side2=bl["side2"][pick],
+                  ibeam=bl["ibeam"][pick], spectrum=load["spectrum"])
+    nplain = int(np.mean(load["nhist"]))
+    eng.run_beamlets(sample, nplain // 10, 10, 1e-4, seed=2, mode=PLAIN_FP64)
+    _, _, _, _, pst = eng.run_beamlets(sample, nplain, 10, 1e-4, seed=3, mode=PLAIN_FP64)
+    plain = pst["histories"] / pst["seconds"]
+    extras["plain_fp64"] = {"value": plain, "unit": "histories/s", "beamlets": m, "histories_per_beamlet": nplain,
+                            "speedup_served_vs_plain": value / plain}
+    # the reference (unmodified matRad entry, OpenMP) on this host's cores
+    from oracle import refbench
+    if refbench.available():
+        cores = host_cores()
+        res = refbench.run_pinned(load["order"][:args.ref_beamlets], load["nhist"][:args.ref_beamlets], cores,
+                                  seed=args.load_seed)
+        r = ref_summary(res)
+        extras["cpu_baseline"] = {"value": r["value"], "unit": "histories/s", "cores": cores, "kind": "reference",
+                                  "sample": f"{len(res)} beamlets of the load, one unmodified matRad-entry call each "
+                                            f"(OpenMP), {r['loop_s']:.1f} s of beamlet loops",
+                                  "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "unc": r["unc"]}
+        one = refbench.run_pinned(load["order"][:args.ref_beamlets_1core], load["nhist"][:args.ref_beamlets_1core],
+                                  1, seed=args.load_seed)
+        r1 = ref_summary(one)
+        extras["cpu_baseline_1core"] = {"value": r1["value"], "unit": "histories/s", "cores": 1, "kind": "reference",
+                                        "sample": f"{len(one)} beamlets, {r1['loop_s']:.1f} s"}
+    else:
+        extras["cpu_baseline"] = None
+    return extras
+
+
+def ref_summary(res):
+    """Histories/s, per-beamlet time percentiles and uncertainty of the
+    reference's beamlet runs (refbench records)."""
+    nh = np.array([r["nhist"] for r in res], dtype=np.float64)
+    ls = np.array([r["loop_s"] for r in res])
+    unc = np.array([r["unc"] for r in res])
+    value = float(nh.sum() / ls.sum())
+    return {"value": value, "loop_s": float(ls.sum()), "p50_ms": float(np.percentile(1e3 * ls, 50)),
+            "p99_ms": float(np.percentile(1e3 * ls, 99)), "unc": unc_summary(unc, nh, value)}
+
+
+def run_reference_beamlets(args):
+    """Reference arm on the beamlet load: the unmodified matRad entry on all
+    host cores, a different sample of the load's beamlets each step (the
+    same beamlets, in the same order, that the GPU arm serves), one call per
+    beamlet as the per-request history counts need."""
+    from oracle import refbench
+    if not refbench.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs an ompMC checkout "
+                                                               "at build time)"}))
+        return 0
+    from ompmc_b200.workloads import LOAD_NBATCH, LOAD_REL, beamlet_load
+    load = beamlet_load(args.load_seed)
+    order, nh = load["order"], load["nhist"]
+    cores = host_cores()
+    S = args.ref_beamlets_per_step
+    n = len(order)
+    for w in range(args.warmup):
+        pos = np.array([n - 1 - w])
+        refbench.run_pinned(order[pos], nh[pos], cores, seed=args.load_seed)
+    res, per_step = [], []
+    for k in range(args.steps):
+        pos = (k * S + np.arange(S)) % n            # requests k*S .. k*S+S-1 of the load
+        r = refbench.run_pinned(order[pos], nh[pos], cores, seed=args.load_seed)
+        res += r
+        per_step.append(sum(x["loop_s"] for x in r))
+    s = ref_summary(res)
+    out = {
+        "metric": METRIC, "value": s["value"], "unit": "histories/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(per_step)), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"],
+        "config": {"workload": WORKLOAD, "beamlets_per_step": S, "nbatch": LOAD_NBATCH, "rel_threshold": LOAD_REL,
+                   "parallelism": f"openmp{cores}", "load_seed": args.load_seed,
+                   "timing": "the beamlet loop of each call (waitbar calls before and after it); table "
+                             "initialisation per call excluded"},
+        "cpu_baseline": {"value": s["value"], "unit": "histories/s", "cores": cores, "kind": "reference",
+                         "sample": f"{S} beamlets of the load per step x {args.steps} steps, unmodified matRad "
+                                   f"entry (OpenMP)"},
+        "e2e": {"value": s["value"], "unit": "histories/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "unc": s["unc"],
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def main_slab64(args):
     serving_params = json.loads(args.serving_params) if args.serving_params else None
     if args.serving_only:
         print(json.dumps({"serving": bench_serving(int(os.environ.get("LOCAL_RANK", "0")), args.serving_requests,
@@ -556,7 +856,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if mode == EVENT_FP32 else "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "mode": args.mode, "histories_per_step_per_gpu": nstep,
+            "config": {"workload": SLAB_WORKLOAD, "mode": args.mode, "histories_per_step_per_gpu": nstep,
                        "tally": "f64", "parallelism": f"replicas{world}", "tuned": tuned,
                        "l2": "particle queues (0.8 GB) and batch tallies exceed L2; physics tables are L2-resident"},
             "e2e": {"value": e2e, "unit": "histories/s", "h2d_bytes_per_step": 2 * 1000 * 8 + 64,
@@ -570,6 +870,47 @@ def main():
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="beamlets", choices=["beamlets", "slab64"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the comparators (CPU reference, plain form)")
+    # beamlet load
+    ap.add_argument("--load-seed", type=int, default=7, help="seed of the request order, histories and arrivals")
+    ap.add_argument("--arrival-rate", type=float, default=4000.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--latency-load", type=float, default=0.7,
+                    help="offered load of the latency pass, as a fraction of the measured throughput")
+    ap.add_argument("--profile-requests", type=int, default=400, help="requests of the profiled pass")
+    ap.add_argument("--plain-sample", type=int, default=12, help="beamlets of the plain FP64 comparator")
+    ap.add_argument("--ref-beamlets", type=int, default=24, help="beamlets of the CPU baseline (all cores)")
+    ap.add_argument("--ref-beamlets-1core", type=int, default=2, help="beamlets of the 1-core CPU baseline")
+    ap.add_argument("--ref-beamlets-per-step", type=int, default=16, help="reference arm: beamlets per step")
+    # slab64 dose run
+    ap.add_argument("--mode", default="event", choices=["event", "plain"])
+    ap.add_argument("--hist-per-step", type=int, default=HIST_PER_STEP)
+    ap.add_argument("--ref-sample", type=int, default=10_000_000)
+    ap.add_argument("--serving-requests", type=int, default=300,
+                    help="slab64: beamlet requests in the serving extra (0 skips it)")
+    ap.add_argument("--no-tune", action="store_true", help="slab64: skip the autotuner (default launch parameters)")
+    ap.add_argument("--cycle-trace", action="store_true",
+                    help="slab64: print the per-cycle trace (queue sizes, kernel ms) of the first warm-up step and "
+                         "exit")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="run only the 300-request serving sample and print its JSON object")
+    ap.add_argument("--serving-params", default=None,
+                    help="event-form parameters of the serving engine (and of the --cycle-trace run), as JSON "
+                         "(Engine.event_params keywords)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    if args.workload == "slab64" or args.serving_only or args.cycle_trace:
+        return main_slab64(args)
+    return main_beamlets(args)
 
 
 if __name__ == "__main__":

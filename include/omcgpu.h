@@ -12,7 +12,11 @@
  * explicitly.  Voxel arrays are x-fastest: v = i + j*nx + k*nx*ny, which is
  * ompMC's region number minus one (omc_dosxyz.c:124-128).
  *
- * Threading: one host thread drives an engine at a time.
+ * Threading: one host thread drives an engine at a time, except through a
+ * server: the omc_server_* calls of one server may come from any number of
+ * host threads (they serialise on the server's mutex), so producers can
+ * submit requests while another thread steps the server and collects
+ * results.
  */
 #ifndef OMCGPU_H
 #define OMCGPU_H
@@ -227,8 +231,12 @@ int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, ui
  * lives in one file-scope device array sized for OMC_NOALLOC_MAX_VOXELS
  * voxels (about 10 MB), held by every GPU that loads the library until the
  * process exits.  Phantoms above that size are rejected with OMC_E_RANGE.
- * The first call on a device looks the array's address up
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The first call on a device is a warm-up to make at start-up: it loads the
+ * library's kernels on that device (lazy module loading), which may
+ * allocate, and looks the array's address up (cudaGetSymbolAddress); make
+ * it before any stream capture.  Later calls allocate nothing.  The address
+ * is looked up again when the device's context has changed (after
+ * cudaDeviceReset, for instance). 
  * Every call shares the array and clears it at its start: calls that
  * overlap on the GPU (other threads, other engines on the same device)
  * race.  Arguments and results are those of omc_run_beam with mode
@@ -262,7 +270,9 @@ int omc_run_beamlets(omc_engine *e, const omc_beamlets *b, int64_t nhist, int nb
  * queues, and requests beyond the budget wait and are admitted first come
  * first served as earlier ones finish.  omc_server_* replace the
  * sequential beamlet loop of omc_matrad.c:1576.  OMC_E_NOMEM when the
- * budget holds no request. */
+ * budget holds no request.  Thread-safe: every call on a server holds its
+ * mutex, so submissions from other threads wait for a step in progress
+ * (at most a few transport cycles). */
 typedef struct omc_server omc_server;
 int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint64_t seed, omc_server **out);
 int omc_server_destroy(omc_server *s);
@@ -287,6 +297,21 @@ int omc_server_result_sparse(omc_server *s, int id, int32_t *rows, double *vals,
                              int64_t *nnz);
 int omc_server_result_dense(omc_server *s, int id, double *dose, double *unc);
 int omc_server_release(omc_server *s, int id);
+/* Completion queue (no reference counterpart): copies into ids (capacity
+ * cap) the requests that finished since the previous call, in the order
+ * they finished, and removes them from the queue; *n receives the count. */
+int omc_server_completed(omc_server *s, int *ids, int cap, int *n);
+/* Device time of the server's stream between two marks (no reference
+ * counterpart): stop = 0 records the start mark; stop = 1 records the end
+ * mark, waits for it and returns the milliseconds between them in *ms. */
+int omc_server_timer(omc_server *s, int stop, double *ms);
+/* Counters of a server since its creation (no reference counterpart):
+ * out (n >= 4) = transport cycles, drain launches, kernel launches
+ * (cycles, drains, folds, finalisation and column extraction), requests
+ * finished.  With options.profile = 1 the server launches its cycles one
+ * by one with events around each kernel, and omc_profile_last reports the
+ * per-kernel times and transport counters of everything it has run. */
+int omc_server_stats(omc_server *s, double *out, int n);
 
 /* ---------------------------------------------- drop-in CLI (dosxyz)
  * The whole omc_dosxyz program (omc_dosxyz.c:1072-1307): reads
@@ -309,6 +334,25 @@ int omc_trace_rays(omc_engine *e, const double *rays, int nrays, int cap, double
  * deposits and random numbers consumed. */
 int omc_replay(omc_engine *e, const double *prim, int nhist, const double *rn, const int64_t *rn_off,
                int dep_cap, int32_t *dep_ir, double *dep_e, int32_t *ndep, int64_t *nused, uint32_t *flags);
+
+/* Samplers: runs one FP64 interaction sampler per case on the scripted
+ * uniform stream rn[rn_off[c] .. rn_off[c+1]) of case c, from the particle
+ * q[11*c] (x,y,z,u,v,w,e,wt,ir,iq,dnear; e total energy).  which: 0 compton
+ * (ompmc.c:1688-1801), 1 photo (:1804-1864), 2 pair (:1447-1685),
+ * 3 rayleigh (:1120-1163), 4 moller (:4377-4453), 5 bhabha (:4456-4543),
+ * 6 brems (:4188-4374), 7 annih (:4546-4663), 8 rannih (:4129-4185),
+ * 9 msdist (:3805-3994, with de = extra[2c] and tustep = extra[2c+1]).
+ * out[44*c ...] receives up to 4 particles of 11 doubles: the input particle
+ * after the sampler, then what it pushed (msdist: ustep and the final
+ * x,y,z,u,v,w); nout[c] their number, used[c] the random numbers drawn,
+ * flags[c] device error bits (8: the stream ran out). */
+int omc_kat(omc_engine *e, int which, const double *q, const double *extra, int n, const double *rn,
+            const int64_t *rn_off, double *out, int32_t *nout, int64_t *used, uint32_t *flags);
+
+/* Device allocations (cudaMalloc) the library has made in this process, all
+ * engines and devices together; no reference counterpart.  Tests read it
+ * around a call to show that the call allocated nothing. */
+int64_t omc_device_allocations(void);
 
 #ifdef __cplusplus
 }

@@ -119,6 +119,76 @@ def write_spin_standin(path, zmax=SPIN_ZMAX):
     return path
 
 
+def write_spin_synthetic(path, seed=2024, zmax=SPIN_ZMAX):
+    """Write a seeded, non-constant spin file in the same layout, to exercise
+    the spin-dependent code paths (Mott/spin rejection in the multiple
+    scattering sampler, the first- and second-moment corrections of the MS
+    step): it is test data, not physics.
+
+    For element Z, charge q, energy index i and q-index j, the surface over
+    the 32 u-nodes k is the smooth, strictly positive
+        s(k) = 1 - a * (1 - cos(pi * k / 31)) / 2 * (1 + b * sin(pi * k / 11)),
+    a in [0.1, 0.6] and b in [-0.15, 0.15] varying smoothly with (Z, q, i, j)
+    plus a seeded random part; fmax[j] in [0.6, 1.4]; dum1, dum3 (first-moment
+    factors) within 8 % of 1 and dum2 within 6 % of the neutral gamma(eta),
+    so the q1 and q2 corrections differ from 1."""
+    rng = np.random.default_rng(seed)
+    espin_min, espin_max = SPIN_ESPIN_MIN_KEV, SPIN_ESPIN_MAX_KEV
+    tau_max = espin_max / (1000.0 * RM)
+    b2min = tau_max * (tau_max + 2.0) / (tau_max + 1.0) ** 2
+    b2max = SPIN_B2_MAX
+    earray = _spin_energy_grid(espin_min, espin_max, np.float32(b2min), np.float32(b2max))
+    nrec = 1 + zmax * 64
+    buf = bytearray(nrec * _REC_FLOATS * 4)
+    hdr = b"stand-in synthetic spin data v1".ljust(32, b" ") + b"LITL"
+    buf[0:36] = hdr
+    struct.pack_into("<4f", buf, 36, espin_min, espin_max, b2min, b2max)
+    tf = 137.03604 * 0.88534138
+    k = np.arange(32)
+    for z in range(1, zmax + 1):
+        z23 = z ** (2.0 / 3.0)
+        for q in range(2):
+            for i in range(2 * _MXE_SPIN + 2):
+                tau = earray[i] / (1000.0 * RM)
+                eta = z23 / (tf * tf) * SPIN_AUX_O / 4.0 / tau / (tau + 2.0)
+                ph = 0.37 * z + 1.3 * q + 0.21 * i
+                dum1 = 1.0 + 0.05 * math.sin(ph) + 0.03 * (rng.random() - 0.5)
+                dum3 = 1.0 + 0.04 * math.cos(0.5 * ph) + 0.03 * (rng.random() - 0.5)
+                dum2 = _gamma_of_eta(eta) * (1.0 + 0.05 * math.sin(0.7 * ph + 0.4) + 0.02 * (rng.random() - 0.5))
+                rec = 1 + (z - 1) * 64 + 32 * q + i
+                off = rec * _REC_FLOATS * 4
+                struct.pack_into("<4f", buf, off, dum1, dum2, dum3, SPIN_AUX_O)
+                fmax = 0.6 + 0.8 * rng.random(16)
+                buf[off + 16: off + 80] = struct.pack("<16f", *fmax)
+                surf = np.zeros((16, 32))
+                for j in range(16):
+                    a = 0.35 + 0.25 * math.sin(0.11 * z + 0.9 * q + 0.17 * i + 0.29 * j) * 0.8 + 0.1 * rng.random()
+                    a = min(max(a, 0.1), 0.6)
+                    b = 0.15 * math.sin(0.3 * i + 0.7 * j + q)
+                    surf[j] = 1.0 - a * (1.0 - np.cos(np.pi * k / 31.0)) / 2.0 * (1.0 + b * np.sin(np.pi * k / 11.0))
+                u16 = np.clip(np.round(surf * 65535.0), 1, 65535).astype(np.uint16)
+                buf[off + 80: off + 80 + 1024] = u16.tobytes()
+    Path(path).parent.mkdir(parents=True, exist_ok=True)
+    with open(path, "wb") as f:
+        f.write(bytes(buf))
+    return path
+
+
+def stage_spin_variant(root=ASSETS):
+    """A second data folder, `data_spin/`, holding the same cross-section and
+    multiple-scattering files and the synthetic spin file; returns it."""
+    root = Path(root)
+    src = require_assets(root) / "data"
+    dst = root / "data_spin"
+    if (dst / "spinms.data").exists() and all((dst / f).exists() for f in DATA_FILES):
+        return dst
+    dst.mkdir(parents=True, exist_ok=True)
+    for f in DATA_FILES:
+        shutil.copyfile(src / f, dst / f)
+    write_spin_synthetic(dst / "spinms.data")
+    return dst
+
+
 # --------------------------------------------------------------------------
 # Staging of the physics data shipped by ompMC
 # --------------------------------------------------------------------------
@@ -134,15 +204,22 @@ def assets_ready(root=ASSETS):
     return all(p.exists() for p in need)
 
 
-def stage(reference_root="/root/reference", root=ASSETS, force=False):
+def stage(reference_root=None, root=ASSETS, force=False):
     """Copy ompMC's physics data into `root` and write the stand-in spin file.
 
-    Returns the assets root.  Raises FileNotFoundError when neither the
-    staged files nor an ompMC checkout are available.
+    `reference_root` is an ompMC checkout (default: the OMPMC_REFERENCE
+    environment variable).  Returns the assets root.  Raises
+    FileNotFoundError when neither the staged files nor an ompMC checkout
+    are available.
     """
     root = Path(root)
     if assets_ready(root) and not force:
         return root
+    if reference_root is None:
+        reference_root = os.environ.get("OMPMC_REFERENCE", "")
+    if not reference_root:
+        raise FileNotFoundError(f"physics data not staged under {root}; pass an ompMC checkout "
+                                "(stage(reference_root=...) or OMPMC_REFERENCE)")
     ref = Path(reference_root)
     if not (ref / "data").is_dir():
         raise FileNotFoundError(
@@ -161,10 +238,11 @@ def stage(reference_root="/root/reference", root=ASSETS, force=False):
 
 
 def require_assets(root=ASSETS):
-    """Return the assets root, staging it from an ompMC checkout if needed."""
-    if assets_ready(root):
-        return Path(root)
-    return stage(root=root)
+    """Return the assets root, staging it from an ompMC checkout if needed
+    (its `out` folder, where runs write their outputs, is created)."""
+    root = Path(root) if assets_ready(root) else stage(root=root)
+    (root / "out").mkdir(parents=True, exist_ok=True)
+    return root
 
 
 # --------------------------------------------------------------------------

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -65,6 +66,8 @@ extern "C" int omc_dosxyz_run(const char *inp_base, const char *out_name, int mo
     data = strip_spaces(data);
     if ((rc = omc_tables_build(pegs.c_str(), pgs4.c_str(), data.c_str(), media.data(), (int)media.size(), &tab)))
         return fail(rc, omc_last_error());
+    // the table set is released on every return below
+    std::unique_ptr<omc_tables, void (*)(omc_tables *)> tab_guard(tab, omc_tables_free);
 
     omc_options opt;
     omc_options_default(&opt);
@@ -82,7 +85,6 @@ extern "C" int omc_dosxyz_run(const char *inp_base, const char *out_name, int mo
     if (in.get("spectrum file", v)) {
         int n = 0;
         if ((rc = omc_spectrum_load(strip_spaces(v).c_str(), cdf1.data(), cdf2.data(), &n))) {
-            omc_tables_free(tab);
             return fail(rc, omc_last_error());
         }
         beam.energy.n = n;
@@ -90,28 +92,23 @@ extern "C" int omc_dosxyz_run(const char *inp_base, const char *out_name, int mo
         beam.energy.cdf2 = cdf2.data();
     } else {
         if (!need(in, "mono energy", v)) {
-            omc_tables_free(tab);
             return fail(OMC_E_ARG, "Can not find 'mono energy' key on input file.");
         }
         beam.energy.mono_energy = std::atof(v.c_str());
     }
     if (!need(in, "collimator bounds", v) ||
         std::sscanf(v.c_str(), "%lf %lf %lf %lf", &beam.xinl, &beam.xinu, &beam.yinl, &beam.yinu) != 4) {
-        omc_tables_free(tab);
         return fail(OMC_E_ARG, "Can not find 'collimator bounds' key on input file.");
     }
     if (!need(in, "charge", v)) {
-        omc_tables_free(tab);
         return fail(OMC_E_ARG, "Can not find 'charge' key on input file.");
     }
     beam.energy.charge = std::atoi(v.c_str());
     if (!need(in, "ssd", v)) {
-        omc_tables_free(tab);
         return fail(OMC_E_ARG, "Can not find 'ssd' key on input file.");
     }
     beam.ssd = std::atof(v.c_str());
     if (beam.ssd < 0) {
-        omc_tables_free(tab);
         return fail(OMC_E_ARG, "SSD must be greater than zero.");
     }
     long ncase = 0;
@@ -129,7 +126,6 @@ extern "C" int omc_dosxyz_run(const char *inp_base, const char *out_name, int mo
     omc_phantom P{ph.nx, ph.ny, ph.nz, ph.xb.data(), ph.yb.data(), ph.zb.data(), ph.med.data(), ph.rho.data()};
     omc_engine *eng = nullptr;
     if ((rc = omc_engine_create(tab, &P, &opt, &eng))) {
-        omc_tables_free(tab);
         return fail(rc, omc_last_error());
     }
     std::vector<double> dose(ph.nvox()), unc(ph.nvox());
@@ -138,7 +134,6 @@ extern "C" int omc_dosxyz_run(const char *inp_base, const char *out_name, int mo
     if (rc) {
         std::string m = omc_engine_last_error(eng);
         omc_engine_destroy(eng);
-        omc_tables_free(tab);
         return fail(rc, m);
     }
     if (verbose) {
@@ -149,6 +144,5 @@ extern "C" int omc_dosxyz_run(const char *inp_base, const char *out_name, int mo
     }
     rc = write_3ddose(strip_spaces(outdir) + out_name + ".3ddose", ph, dose, unc);
     omc_engine_destroy(eng);
-    omc_tables_free(tab);
     return rc;
 }

@@ -1,6 +1,7 @@
 // Engine: resident device tables and phantom, batch statistics, and the C
 // ABI entry points of include/omcgpu.h.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -25,6 +26,9 @@ int global_err(int code, const std::string &msg) {
 
 namespace omc {
 
+// Device allocations the library has made (every one goes through DBuf).
+static std::atomic<long long> g_device_allocs{0};
+
 int DBuf::alloc(size_t bytes) {
     release();
     if (bytes == 0) bytes = 16;
@@ -34,6 +38,7 @@ int DBuf::alloc(size_t bytes) {
         return rc == cudaErrorMemoryAllocation ? OMC_E_NOMEM : OMC_E_CUDA;
     }
     n = bytes;
+    g_device_allocs.fetch_add(1, std::memory_order_relaxed);
     return OMC_OK;
 }
 
@@ -400,6 +405,8 @@ const char *omc_last_error(void) {
 
 int omc_version(void) { return 10000; }
 
+int64_t omc_device_allocations(void) { return g_device_allocs.load(std::memory_order_relaxed); }
+
 int omc_tables_build(const char *pegs_file, const char *pgs4form_file, const char *data_folder,
                      const char *const *media, int nmed, omc_tables **out) {
     if (!pegs_file || !pgs4form_file || !data_folder || !media || !out || nmed <= 0)
@@ -667,11 +674,12 @@ int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, ui
         cudaEventCreate(&t1);
         cudaEventRecord(t0, e->stream);
         for (int ib = 0; ib < nbatch; ib++) {
+            long nl = 0;
             if ((rc = plain_beam_batch(e, S, work.as<double>(), seed, (long)ib * nper, nper, acc.as<double>() + 1,
-                                       block)))
+                                       block, &nl)))
                 return rc;
             if ((rc = fold(e, work.as<double>(), sum.as<double>(), sum2.as<double>(), nv, 1.0))) return rc;
-            ks.launches += 2;
+            ks.launches += nl + 1;
         }
         cudaEventRecord(t1, e->stream);
         if ((rc = cuda_check(e, cudaEventSynchronize(t1), "beam transport"))) return rc;
@@ -759,6 +767,37 @@ int omc_replay(omc_engine *e, const double *prim, int nhist, const double *rn, c
     cudaMemcpyAsync(nused, nu.p, nhist * 8, cudaMemcpyDeviceToHost, e->stream);
     cudaMemcpyAsync(flags, fl.p, nhist * 4, cudaMemcpyDeviceToHost, e->stream);
     return cuda_check(e, cudaStreamSynchronize(e->stream), "omc_replay");
+}
+
+int omc_kat(omc_engine *e, int which, const double *q, const double *extra, int n, const double *rn,
+            const int64_t *rn_off, double *out, int32_t *nout, int64_t *used, uint32_t *flags) {
+    if (!e || !q || n <= 0 || !rn || !rn_off || !out || !nout || !used || !flags || which < 0 || which > KAT_MSDIST ||
+        (which == KAT_MSDIST && !extra))
+        return global_err(OMC_E_ARG, "omc_kat: bad argument");
+    cudaSetDevice(e->device);
+    const long nvox = e->ph.nvox();
+    for (int c = 0; c < n; c++)
+        if (q[11 * c + 8] < 1 || q[11 * c + 8] > nvox) return set_err(e, OMC_E_ARG, "omc_kat: region out of range");
+    long nrn = rn_off[n];
+    DBuf qd, xd, rd, od, outd, nd, ud, fd;
+    int rc;
+    if ((rc = qd.alloc((size_t)n * 11 * 8)) || (rc = xd.alloc((size_t)n * 2 * 8)) ||
+        (rc = rd.alloc(std::max(1L, nrn) * 8)) || (rc = od.alloc((size_t)(n + 1) * 8)) ||
+        (rc = outd.alloc((size_t)n * KAT_MAXOUT * 11 * 8)) || (rc = nd.alloc((size_t)n * 4)) ||
+        (rc = ud.alloc((size_t)n * 8)) || (rc = fd.alloc((size_t)n * 4)))
+        return set_err(e, rc, "alloc");
+    cudaMemcpyAsync(qd.p, q, (size_t)n * 11 * 8, cudaMemcpyHostToDevice, e->stream);
+    if (extra) cudaMemcpyAsync(xd.p, extra, (size_t)n * 2 * 8, cudaMemcpyHostToDevice, e->stream);
+    if (nrn > 0) cudaMemcpyAsync(rd.p, rn, nrn * 8, cudaMemcpyHostToDevice, e->stream);
+    cudaMemcpyAsync(od.p, rn_off, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice, e->stream);
+    if ((rc = plain_kat(e, which, qd.as<double>(), xd.as<double>(), n, rd.as<double>(), od.as<long>(),
+                        outd.as<double>(), nd.as<int>(), ud.as<long>(), fd.as<unsigned>())))
+        return rc;
+    cudaMemcpyAsync(out, outd.p, (size_t)n * KAT_MAXOUT * 11 * 8, cudaMemcpyDeviceToHost, e->stream);
+    cudaMemcpyAsync(nout, nd.p, (size_t)n * 4, cudaMemcpyDeviceToHost, e->stream);
+    cudaMemcpyAsync(used, ud.p, (size_t)n * 8, cudaMemcpyDeviceToHost, e->stream);
+    cudaMemcpyAsync(flags, fd.p, (size_t)n * 4, cudaMemcpyDeviceToHost, e->stream);
+    return cuda_check(e, cudaStreamSynchronize(e->stream), "omc_kat");
 }
 
 }  // extern "C"

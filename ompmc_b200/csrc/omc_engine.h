@@ -96,8 +96,10 @@ int set_err(omc_engine *e, int code, const std::string &msg);
 int cuda_check(omc_engine *e, cudaError_t rc, const char *what);
 
 // Plain FP64 form (omc_plain.cu).
+// *launches (may be null) receives the kernel launches made: a batch is
+// split into launches of at most a few million histories.
 int plain_beam_batch(omc_engine *e, const BeamSrc<double> &S, double *work, uint64_t seed, long hist0, long n,
-                     double *src_energy, int block);
+                     double *src_energy, int block, long *launches = nullptr);
 int plain_beamlet_batch(omc_engine *e, const BeamletSrc<double> &S, int ib, double *work, uint64_t seed, long hist0,
                         long n, int block);
 int plain_trace(omc_engine *e, const double *rays_d, int nrays, int cap, double *ustep, int *irnew, int *idisc,
@@ -107,4 +109,10 @@ int plain_trace(omc_engine *e, const double *rays_d, int nrays, int cap, double 
 size_t plain_replay_stack_bytes(int nhist);
 int plain_replay(omc_engine *e, const double *prim, int nhist, const double *rn, const long *rn_off, int dep_cap,
                  int *dep_ir, double *dep_e, int *ndep, long *nused, unsigned *flags, void *stacks);
+// Sampler known-answer hook (omc_kat): `out` holds KAT_MAXOUT particles of
+// 11 doubles per case.
+constexpr int KAT_MAXOUT = 4;
+constexpr int KAT_MSDIST = 9;
+int plain_kat(omc_engine *e, int which, const double *q, const double *extra, int n, const double *rn,
+              const long *rn_off, double *out, int *nout, long *used, unsigned *flags);
 }  // namespace omc

@@ -1141,6 +1141,52 @@ void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, in
     launch_transport(e, iph, iel, oph, oel, tallies, seedw, sd->live, nbmax, nullptr);
 }
 
+// A serving cycle launched on its own with an event around each kernel
+// (engines created with options.profile): the per-kernel device time is
+// added to the engine's profile; the transport counters are those the
+// control block has accumulated since the server was created.
+int serve_profiled_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target) {
+    EventState &S = *e->ev;
+    int iph = in == 0 ? 0 : 2, iel = iph + 1;
+    int oph = in == 0 ? 2 : 0, oel = oph + 1;
+    const uint32_t seedw = SERVE_SEEDW;
+    cudaEvent_t ev[5];
+    for (auto &x : ev) cudaEventCreate(&x);
+    cudaEventRecord(ev[0], e->stream);
+    k_serve_plan<<<1, 1, 0, e->stream>>>(sd, S.ctl_d, iph, iel, plan_cfg(e, target));
+    cudaEventRecord(ev[1], e->stream);
+    k_serve_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, sd, S.q[iph], S.q[iel], S.ctl_d, nbmax, seedw);
+    cudaEventRecord(ev[2], e->stream);
+    launch_transport(e, iph, iel, oph, oel, tallies, seedw, sd->live, nbmax, ev);
+    cudaEventRecord(ev[4], e->stream);
+    int rc = cuda_check(e, cudaEventSynchronize(ev[4]), "profiled serving cycle");
+    if (!rc) {
+        float t[4];
+        for (int k = 0; k < 4; k++) cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]);
+        const int map[4] = {3, 0, 1, 2};   // plan, source, photon, electron (+ interactions)
+        for (int k = 0; k < 4; k++) {
+            S.prof[map[k]].seconds += t[k] * 1e-3;
+            S.prof[map[k]].launches += 1;
+        }
+        Ctl h{};
+        cudaMemcpy(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
+        for (int k = 0; k < 2; k++) {
+            KernelProfile &P = S.prof[1 + k];
+            P.particles = (double)h.st_events[k];
+            P.steps = (double)h.st_steps[k];
+            P.cross = (double)h.st_cross[k];
+            P.dep = (double)h.st_dep[k];
+            P.atom = (double)h.st_atom[k];
+        }
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+    return rc;
+}
+
+void serve_profile_reset(omc_engine *e) {
+    for (auto &p : e->ev->prof) p = KernelProfile();
+}
+
 // The drain in serving: the particles left in queues A (where a graph of
 // two cycles leaves them) run to the end on the serving streams; then the
 // queues are emptied and every request's live count is zero.

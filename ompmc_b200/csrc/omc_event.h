@@ -139,6 +139,8 @@ int event_interact_queue(omc_engine *e);
 // particle = request slot * nbmax + batch.
 void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
 void serve_drain(omc_engine *e, ServeDev *sd, long long left, double *tallies);
+int serve_profiled_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
+void serve_profile_reset(omc_engine *e);
 // Particles left at or below which a run whose histories are all injected
 // switches from transport cycles to the drain kernel (0: never).
 long long drain_threshold(const omc_engine *e);

@@ -15,7 +15,8 @@
 // OMC_NOALLOC_MAX_VOXELS voxels' worth of tallies (about 10 MB); every GPU
 // that loads the library holds it until the process exits.  Host code never
 // passes the array's name to a kernel (on the host it is only a stand-in):
-// the device address is taken once per device with cudaGetSymbolAddress.
+// the device address is taken once per device with cudaGetSymbolAddress,
+// and again if that device's context has been replaced since.
 #include <chrono>
 #include <mutex>
 
@@ -48,18 +49,40 @@ namespace {
 
 std::mutex g_mu;
 double *g_scratch[64] = {};
+void *g_scratch_ctx[64] = {};
 
-// Device address of the scratch array on the engine's device, looked up on
-// the first call made for that device.
+// The driver's current context (CUcontext) through the runtime's entry-point
+// lookup, so the library needs no link-time dependency on libcuda.
+using CtxGetCurrent = int (*)(void **);
+CtxGetCurrent ctx_get_current() {
+    static CtxGetCurrent fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (CtxGetCurrent)f;
+    }();
+    return fn;
+}
+
+// Device address of the scratch array on the engine's device (which is
+// current), looked up on the first call made for that device and again
+// whenever the device's context is not the one it was looked up in: a
+// context torn down by cudaDeviceReset takes the old address with it.
 int scratch_on(omc_engine *e, double **out) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (e->device < 0 || e->device >= 64) return set_err(e, OMC_E_ARG, "device ordinal out of range");
-    if (!g_scratch[e->device]) {
+    void *ctx = nullptr;
+    CtxGetCurrent get = ctx_get_current();
+    if (!get || get(&ctx) != 0 || !ctx) return set_err(e, OMC_E_CUDA, "no current CUDA context for the scratch lookup");
+    if (!g_scratch[e->device] || g_scratch_ctx[e->device] != ctx) {
         void *p = nullptr;
         cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (rc != cudaSuccess)
             return set_err(e, OMC_E_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(rc));
         g_scratch[e->device] = (double *)p;
+        g_scratch_ctx[e->device] = ctx;
     }
     *out = g_scratch[e->device];
     return OMC_OK;
@@ -92,15 +115,20 @@ extern "C" int omc_run_beam_noalloc(omc_engine *e, const omc_beam *b, int64_t nc
     double *work = s + OFF_WORK, *sum = s + OFF_SUM, *sum2 = s + OFF_SUM2;
     double *dose_d = s + OFF_DOSE, *unc_d = s + OFF_UNC, *cdf = s + OFF_CDF, *acc = s + OFF_ACC;
     // the array keeps the previous call's contents: clear what accumulates
-    cudaMemsetAsync(work, 0, nv * 8, e->stream);
-    cudaMemsetAsync(sum, 0, nv * 8, e->stream);
-    cudaMemsetAsync(sum2, 0, nv * 8, e->stream);
-    cudaMemsetAsync(acc, 0, 8 * 8, e->stream);
-    cudaMemsetAsync(e->errword.p, 0, sizeof(unsigned), e->stream);
+    if ((rc = cuda_check(e, cudaMemsetAsync(work, 0, nv * 8, e->stream), "clear scratch")) ||
+        (rc = cuda_check(e, cudaMemsetAsync(sum, 0, nv * 8, e->stream), "clear scratch")) ||
+        (rc = cuda_check(e, cudaMemsetAsync(sum2, 0, nv * 8, e->stream), "clear scratch")) ||
+        (rc = cuda_check(e, cudaMemsetAsync(acc, 0, 8 * 8, e->stream), "clear scratch")) ||
+        (rc = cuda_check(e, cudaMemsetAsync(e->errword.p, 0, sizeof(unsigned), e->stream), "clear error flags")))
+        return rc;
     BeamSrc<double> S = beam_setup<double>(e, b);
     if (ncdf > 0) {
-        cudaMemcpyAsync(cdf, b->energy.cdf1, ncdf * 8, cudaMemcpyHostToDevice, e->stream);
-        cudaMemcpyAsync(cdf + MAXCDF, b->energy.cdf2, ncdf * 8, cudaMemcpyHostToDevice, e->stream);
+        if ((rc = cuda_check(e, cudaMemcpyAsync(cdf, b->energy.cdf1, ncdf * 8, cudaMemcpyHostToDevice, e->stream),
+                             "spectrum upload")) ||
+            (rc = cuda_check(e, cudaMemcpyAsync(cdf + MAXCDF, b->energy.cdf2, ncdf * 8, cudaMemcpyHostToDevice,
+                                                e->stream),
+                             "spectrum upload")))
+            return rc;
         S.cdf1 = cdf;
         S.cdf2 = cdf + MAXCDF;
     } else {
@@ -108,9 +136,11 @@ extern "C" int omc_run_beam_noalloc(omc_engine *e, const omc_beam *b, int64_t nc
     }
     int block = e->opt.block > 0 ? e->opt.block : 128;
     auto t0 = std::chrono::steady_clock::now();
+    long launches = 0;  // transport and fold launches, counted as omc_run_beam counts them
     for (int ib = 0; ib < nbatch; ib++) {
-        if ((rc = plain_beam_batch(e, S, work, seed, (long)ib * nper, nper, acc + 1, block))) return rc;
+        if ((rc = plain_beam_batch(e, S, work, seed, (long)ib * nper, nper, acc + 1, block, &launches))) return rc;
         if ((rc = fold(e, work, sum, sum2, nv, 1.0))) return rc;
+        launches++;
     }
     if ((rc = device_sum(e, sum, nv, acc))) return rc;
     if ((rc = finalize_dosxyz(e, sum, sum2, nbatch, (double)nper, dose_d, unc_d))) return rc;
@@ -125,7 +155,7 @@ extern "C" int omc_run_beam_noalloc(omc_engine *e, const omc_beam *b, int64_t nc
     if (stats) {
         stats[0] = (double)nper * nbatch;
         stats[1] = secs;
-        stats[2] = 2.0 * nbatch + 2;
+        stats[2] = (double)launches;
         stats[3] = a[0];
         stats[4] = a[1];
         stats[5] = (double)flags;

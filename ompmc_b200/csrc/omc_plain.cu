@@ -376,9 +376,10 @@ static int grid_for(omc_engine *e, long n, int block) {
 static const long PLAIN_CHUNK = 1L << 22;
 
 int plain_beam_batch(omc_engine *e, const BeamSrc<double> &S, double *work, uint64_t seed, long hist0, long n,
-                     double *src_energy, int block) {
+                     double *src_energy, int block, long *launches) {
     const bool split = e->d64.d.nsplit > 1;
     for (long c0 = 0; c0 < n; c0 += PLAIN_CHUNK) {
+        if (launches) ++*launches;
         long c = std::min(PLAIN_CHUNK, n - c0);
         if (split)
             k_plain_beam<SPLIT_STACK><<<grid_for(e, c, block), block, 0, e->stream>>>(
@@ -419,6 +420,90 @@ int plain_replay(omc_engine *e, const double *prim, int nhist, const double *rn,
     k_replay<<<(nhist + 63) / 64, 64, 0, e->stream>>>(e->d64.d, prim, nhist, rn, rn_off, dep_cap, dep_ir, dep_e, ndep,
                                                       nused, flags, (Part<double> *)stacks);
     return cuda_check(e, cudaGetLastError(), "k_replay launch");
+}
+
+// ------------------------------------------ sampler known-answer hooks
+// One interaction sampler (or one msdist step) per case on a scripted
+// uniform stream, with the FP64 physics of this translation unit (no
+// contracted multiply-adds, like the x86 reference).  The particle itself
+// is output 0, what the sampler pushes follows.
+struct KatEnv {
+    static constexpr bool kRefOrder = true;
+    ScriptRng rng;
+    Part<double> out[KAT_MAXOUT];
+    int nout;
+    unsigned flags;
+    long work;
+    double edep;
+    __device__ bool tick() { return ++work < HISTORY_BUDGET; }
+    __device__ double uni() { return rng.uni(); }
+    __device__ void deposit(int, double e) { edep += e; }
+    __device__ bool push(const Part<double> &q) {
+        if (nout + 1 >= KAT_MAXOUT) {
+            flags |= ERR_STACK;
+            return false;
+        }
+        out[++nout] = q;
+        return true;
+    }
+    __device__ void err(unsigned f) { flags |= f; }
+    __device__ void cross() {}
+    __device__ bool tstep_take() const { return true; }
+};
+
+__global__ void k_kat(DevData<double> D, int which, const double *q, const double *extra, int n, const double *rn,
+                      const long *rn_off, double *out, int *nout, long *used, unsigned *flags) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double *a = q + 11 * (long)c;
+    Part<double> p{a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], (int)a[8], (int)a[9]};
+    KatEnv g;
+    unsigned fl = 0;
+    g.rng = ScriptRng{rn + rn_off[c], rn_off[c + 1] - rn_off[c], 0, &fl};
+    g.nout = 0;
+    g.flags = 0;
+    g.work = 0;
+    g.edep = 0.0;
+    double *o = out + (long)c * KAT_MAXOUT * 11;
+    for (int k = 0; k < KAT_MAXOUT * 11; k++) o[k] = 0.0;
+    const int imed = p.ir > 0 ? D.med[p.ir] : 0;
+    if (which == KAT_MSDIST) {
+        double xf, yf, zf, uf, vf, wf;
+        double ustep = msdist(D, g, p, imed, p.iq, D.rhof[p.ir], extra[2 * c], extra[2 * c + 1], p.e - D_RM, xf, yf, zf,
+                              uf, vf, wf);
+        double r[7] = {ustep, xf, yf, zf, uf, vf, wf};
+        for (int k = 0; k < 7; k++) o[k] = r[k];
+        nout[c] = 1;
+    } else {
+        const double gle = log(p.e);
+        switch (which) {
+        case 0: compton(D, g, p); break;
+        case 1: photo(D, g, p); break;
+        case 2: pair(D, g, p, imed); break;
+        case 3: rayleigh(D, g, p, imed, gle, lidx(D.ms[imed].ge1, D.ms[imed].ge0, gle)); break;
+        case 4: moller(D, g, p); break;
+        case 5: bhabha(D, g, p); break;
+        case 6: brems(D, g, p); break;
+        case 7: annih(D, g, p); break;
+        case 8: rannih(D, g, p); break;
+        default: g.flags |= ERR_LOOP; break;
+        }
+        g.out[0] = p;
+        for (int i = 0; i <= g.nout; i++) {
+            const Part<double> &t = g.out[i];
+            double r[10] = {t.x, t.y, t.z, t.u, t.v, t.w, t.e, t.wt, (double)t.ir, (double)t.iq};
+            for (int k = 0; k < 10; k++) o[11 * i + k] = r[k];
+        }
+        nout[c] = g.nout + 1;
+    }
+    used[c] = g.rng.pos;
+    flags[c] = g.flags | fl;
+}
+
+int plain_kat(omc_engine *e, int which, const double *q, const double *extra, int n, const double *rn,
+              const long *rn_off, double *out, int *nout, long *used, unsigned *flags) {
+    k_kat<<<(n + 63) / 64, 64, 0, e->stream>>>(e->d64.d, which, q, extra, n, rn, rn_off, out, nout, used, flags);
+    return cuda_check(e, cudaGetLastError(), "k_kat launch");
 }
 
 }  // namespace omc

@@ -20,6 +20,7 @@
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 
 #include "omc_event.h"
 #include "omc_rng.cuh"
@@ -194,6 +195,10 @@ struct Request {
 }  // namespace
 
 struct omc_server {
+    // Guards everything below: submissions may come from any host thread
+    // while one thread steps the server (a matRad-side producer beside the
+    // driving loop); every omc_server_* call holds it for its duration.
+    std::mutex mu;
     omc_engine *e = nullptr;
     int nbmax = 10, nslots = 0;
     long long target = 0;
@@ -207,7 +212,9 @@ struct omc_server {
     std::map<const omc_beamlets *, std::unique_ptr<PlanBuf>> plans;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    long long cycles = 0, drains = 0;
+    long long cycles = 0, drains = 0, launches = 0, finished = 0;
+    std::vector<int> completed;  // finished since the last omc_server_completed
+    cudaEvent_t t_start = nullptr, t_stop = nullptr;
     // state after the last step: particles in the queues, and whether every
     // running request had all its histories injected
     long long left = 0;
@@ -230,6 +237,7 @@ int finalize_request(omc_server *s, Request &r) {
     cudaMemsetAsync(s->f_sum, 0, nv * 8, e->stream);
     cudaMemsetAsync(s->f_sum2, 0, nv * 8, e->stream);
     double scale = r.kind == 1 ? 1.0 / (double)r.nper : 1.0;
+    s->launches += r.nbatch + (r.kind == 0 ? 1 : 5);   // folds, finalise (+ column extraction)
     for (int b = 0; b < r.nbatch; b++) {
         double *w = s->tallies.as<double>() + ((size_t)r.slot * s->nbmax + b) * nv;
         if ((rc = fold(e, w, s->f_sum, s->f_sum2, nv, scale))) return rc;
@@ -365,6 +373,7 @@ int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint6
     s->f_total = (long long *)(s->f_dmax + 1);
     s->slot_req.assign(s->nslots, -1);
     s->target = std::min<long long>((long long)e->ev->cap / 2, e->ev->inflight);
+    if (e->opt.profile) serve_profile_reset(e);
     // reset queue counters and capture two cycles as a graph
     Ctl c0{};
     cudaMemcpyAsync(e->ev->ctl_d, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, e->stream);
@@ -381,12 +390,51 @@ int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint6
 
 int omc_server_destroy(omc_server *s) {
     if (!s) return OMC_OK;
+    { std::lock_guard<std::mutex> lk(s->mu); }  // wait for a call in progress
     cudaSetDevice(s->e->device);
     cudaStreamSynchronize(s->e->stream);
     if (s->exec) cudaGraphExecDestroy(s->exec);
     if (s->graph) cudaGraphDestroy(s->graph);
+    if (s->t_start) cudaEventDestroy(s->t_start);
+    if (s->t_stop) cudaEventDestroy(s->t_stop);
     delete s;
     return OMC_OK;
+}
+
+int omc_server_completed(omc_server *s, int *ids, int cap, int *n) {
+    if (!s || !n || cap < 0 || (cap > 0 && !ids)) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    int k = std::min<int>(cap, (int)s->completed.size());
+    std::copy(s->completed.begin(), s->completed.begin() + k, ids);
+    s->completed.erase(s->completed.begin(), s->completed.begin() + k);
+    *n = k;
+    return OMC_OK;
+}
+
+int omc_server_stats(omc_server *s, double *out, int n) {
+    if (!s || !out || n < 4) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    out[0] = (double)s->cycles;
+    out[1] = (double)s->drains;
+    out[2] = (double)s->launches;
+    out[3] = (double)s->finished;
+    return OMC_OK;
+}
+
+int omc_server_timer(omc_server *s, int stop, double *ms) {
+    if (!s) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    omc_engine *e = s->e;
+    cudaSetDevice(e->device);
+    if (!s->t_start && (cudaEventCreate(&s->t_start) != cudaSuccess || cudaEventCreate(&s->t_stop) != cudaSuccess))
+        return set_err(e, OMC_E_CUDA, "server timer events");
+    if (!stop) return cuda_check(e, cudaEventRecord(s->t_start, e->stream), "server timer start");
+    int rc = cuda_check(e, cudaEventRecord(s->t_stop, e->stream), "server timer stop");
+    if (!rc) rc = cuda_check(e, cudaEventSynchronize(s->t_stop), "server timer stop");
+    float m = 0;
+    if (!rc) rc = cuda_check(e, cudaEventElapsedTime(&m, s->t_start, s->t_stop), "server timer");
+    if (ms) *ms = m;
+    return rc;
 }
 
 static int submit(omc_server *s, std::unique_ptr<Request> r, uint64_t seed) {
@@ -407,9 +455,11 @@ static int submit(omc_server *s, std::unique_ptr<Request> r, uint64_t seed) {
 int omc_server_submit_beamlet(omc_server *s, const omc_beamlets *b, int ibixel, int64_t nhist, int nbatch,
                               double rel_threshold, uint64_t seed) {
     if (!s || !b) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
     int rc = check_beamlets(s->e, b);
     if (rc) return rc;
     if (ibixel < 0 || ibixel >= b->nbixels) return set_err(s->e, OMC_E_ARG, "bixel index out of range");
+    cudaSetDevice(s->e->device);
     if (!s->plans.count(b)) {
         auto p = std::make_unique<PlanBuf>();
         if ((rc = upload_plan<float>(s->e, b, p->f32, p->s32))) return rc;
@@ -427,6 +477,8 @@ int omc_server_submit_beamlet(omc_server *s, const omc_beamlets *b, int ibixel, 
 
 int omc_server_submit_beam(omc_server *s, const omc_beam *b, int64_t nhist, int nbatch, uint64_t seed) {
     if (!s || !b) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    cudaSetDevice(s->e->device);
     auto r = std::make_unique<Request>();
     r->kind = 0;
     r->beam = *b;
@@ -447,19 +499,31 @@ int omc_server_submit_beam(omc_server *s, const omc_beam *b, int64_t nhist, int 
 
 int omc_server_step(omc_server *s, int cycles, int *active) {
     if (!s) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
     omc_engine *e = s->e;
     cudaSetDevice(e->device);
     int rc = admit(s);
     if (rc) return rc;
     if (!s->order.empty()) {
         const long long dthr = drain_threshold(e);
+        const int per_cycle = e->d32.d.defer_interact ? 5 : 4;
         if (dthr > 0 && s->injected && s->pending.empty() && s->left > 0 && s->left <= dthr) {
             serve_drain(e, s->sd, s->left, s->tallies.as<double>());
             s->drains++;
+            s->launches++;
+        } else if (e->opt.profile) {
+            // cycles one by one, timed per kernel (the graph's two cycles)
+            int graphs = std::max(1, cycles / 2);
+            for (int k = 0; k < 2 * graphs; k++)
+                if ((rc = serve_profiled_cycle(e, k & 1, s->sd, s->tallies.as<double>(), s->nbmax, s->target)))
+                    return rc;
+            s->cycles += 2 * graphs;
+            s->launches += 2 * graphs * per_cycle;
         } else {
             int graphs = std::max(1, cycles / 2);
             for (int k = 0; k < graphs; k++) cudaGraphLaunch(s->exec, e->stream);
             s->cycles += 2 * graphs;
+            s->launches += 2 * graphs * per_cycle;
         }
         // completion check: all injected and nothing left in the queues
         std::vector<ServeReq> rq(s->nslots);
@@ -486,6 +550,8 @@ int omc_server_step(omc_server *s, int cycles, int *active) {
                 if ((rc = finalize_request(s, r))) return rc;
                 r.state = 2;
                 r.t_done = now_ms();
+                s->completed.push_back(r.id);
+                s->finished++;
                 s->slot_req[slot] = -1;
                 ServeReq q{};
                 q.kind = -1;
@@ -509,7 +575,9 @@ int omc_server_step(omc_server *s, int cycles, int *active) {
 }
 
 int omc_server_poll(omc_server *s, int id, double *latency_ms) {
-    if (!s || id < 0 || id >= (int)s->reqs.size()) return OMC_E_ARG;
+    if (!s) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (id < 0 || id >= (int)s->reqs.size()) return OMC_E_ARG;
     Request &r = *s->reqs[id];
     if (r.state < 2) return OMC_E_NOTREADY;
     if (latency_ms) *latency_ms = r.t_done - r.t_submit;
@@ -518,7 +586,9 @@ int omc_server_poll(omc_server *s, int id, double *latency_ms) {
 
 int omc_server_result_sparse(omc_server *s, int id, int32_t *rows, double *vals, double *var, int64_t cap,
                              int64_t *nnz) {
-    if (!s || id < 0 || id >= (int)s->reqs.size() || !nnz) return OMC_E_ARG;
+    if (!s) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (id < 0 || id >= (int)s->reqs.size() || !nnz) return OMC_E_ARG;
     Request &r = *s->reqs[id];
     if (r.state < 2) return OMC_E_NOTREADY;
     if (r.kind != 1) return set_err(s->e, OMC_E_ARG, "request is not a beamlet");
@@ -531,7 +601,9 @@ int omc_server_result_sparse(omc_server *s, int id, int32_t *rows, double *vals,
 }
 
 int omc_server_result_dense(omc_server *s, int id, double *dose, double *unc) {
-    if (!s || id < 0 || id >= (int)s->reqs.size()) return OMC_E_ARG;
+    if (!s) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (id < 0 || id >= (int)s->reqs.size()) return OMC_E_ARG;
     Request &r = *s->reqs[id];
     if (r.state < 2) return OMC_E_NOTREADY;
     if (r.kind != 0) return set_err(s->e, OMC_E_ARG, "request is not a beam");
@@ -541,7 +613,9 @@ int omc_server_result_dense(omc_server *s, int id, double *dose, double *unc) {
 }
 
 int omc_server_release(omc_server *s, int id) {
-    if (!s || id < 0 || id >= (int)s->reqs.size()) return OMC_E_ARG;
+    if (!s) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (id < 0 || id >= (int)s->reqs.size()) return OMC_E_ARG;
     Request &r = *s->reqs[id];
     if (r.state < 2) return OMC_E_NOTREADY;
     r.state = 3;

@@ -831,27 +831,43 @@ void build_electron_ranges(Tables &t) {
 }  // namespace
 
 // --------------------------------------------------------------- spline
+// Natural cubic spline through (xs, fs), with the elimination order of
+// EGSnrc's set_spline as ompMC has it (ompmc.c:3034-3076), so that the
+// tables built on it (the spin moment corrections) agree bit for bit:
+// forward pass over the slope differences, back substitution, then the
+// polynomial coefficients of each interval.
 void Spline::fit(const std::vector<double> &xs, const std::vector<double> &fs) {
-    int n = (int)xs.size();
+    const int n = (int)xs.size();
     x = xs;
     a.assign(n, 0); b.assign(n, 0); c.assign(n, 0); d.assign(n, 0);
-    std::vector<double> h(n - 1), m(n, 0.0), alpha(n, 0.0), l(n, 1.0), mu(n, 0.0), zz(n, 0.0);
-    for (int i = 0; i < n - 1; i++) h[i] = xs[i + 1] - xs[i];
-    for (int i = 1; i < n - 1; i++)
-        alpha[i] = 3.0 * ((fs[i + 1] - fs[i]) / h[i] - (fs[i] - fs[i - 1]) / h[i - 1]);
-    for (int i = 1; i < n - 1; i++) {
-        l[i] = 2.0 * (xs[i + 1] - xs[i - 1]) - h[i - 1] * mu[i - 1];
-        mu[i] = h[i] / l[i];
-        zz[i] = (alpha[i] - h[i - 1] * zz[i - 1]) / l[i];
+    // interval widths, and the change of slope at each inner node
+    double prev_slope = 0.0;
+    for (int k = 0; k < n - 1; k++) {
+        d[k] = xs[k + 1] - xs[k];
+        const double slope = (fs[k + 1] - fs[k]) / d[k];
+        c[k] = slope - prev_slope;
+        prev_slope = slope;
     }
-    // c holds the quadratic coefficients (second derivative / 2), natural ends
-    std::vector<double> cc(n, 0.0);
-    for (int i = n - 2; i >= 1; i--) cc[i] = zz[i] - mu[i] * cc[i + 1];
-    for (int i = 0; i < n - 1; i++) {
-        a[i] = fs[i];
-        b[i] = (fs[i + 1] - fs[i]) / h[i] - h[i] * (cc[i + 1] + 2.0 * cc[i]) / 3.0;
-        c[i] = cc[i];
-        d[i] = (cc[i + 1] - cc[i]) / (3.0 * h[i]);
+    c[0] = 0.0;
+    c[n - 1] = 0.0;
+    // forward elimination of the tridiagonal system (diagonal into b)
+    double ratio = 0.0, width = 0.0;
+    for (int k = 1; k < n - 1; k++) {
+        c[k] = c[k] + ratio * c[k - 1];
+        b[k] = 2.0 * (xs[k - 1] - xs[k + 1]) - ratio * width;
+        width = d[k];
+        ratio = width / b[k];
+    }
+    // back substitution, from the last inner node down
+    for (int k = n - 2; k >= 1; k--) c[k] = (d[k] * c[k + 1] - c[k]) / b[k];
+    // coefficients of a + q (b + q (c + q d)) on each interval
+    for (int k = 0; k < n - 1; k++) {
+        const double h = d[k];
+        const double dc = c[k + 1] - c[k];
+        d[k] = dc / h;
+        c[k] = 3.0 * c[k];
+        b[k] = (fs[k + 1] - fs[k]) / h - (c[k] + dc) * h;
+        a[k] = fs[k];
     }
 }
 

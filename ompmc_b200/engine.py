@@ -120,6 +120,11 @@ def lib():
         "omc_server_release": ([C.c_void_p, C.c_int], C.c_int),
         "omc_trace_rays": ([C.c_void_p, _dp, C.c_int, C.c_int, _dp, _ip, _ip, _ip, _dp], C.c_int),
         "omc_replay": ([C.c_void_p, _dp, C.c_int, _dp, _lp, C.c_int, _ip, _dp, _ip, _lp, _up], C.c_int),
+        "omc_device_allocations": ([], C.c_int64),
+        "omc_kat": ([C.c_void_p, C.c_int, _dp, _dp, C.c_int, _dp, _lp, _dp, _ip, _lp, _up], C.c_int),
+        "omc_server_completed": ([C.c_void_p, _ip, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "omc_server_timer": ([C.c_void_p, C.c_int, _dp], C.c_int),
+        "omc_server_stats": ([C.c_void_p, _dp, C.c_int], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name, None)
@@ -129,6 +134,11 @@ def lib():
         f.restype = res
     _lib = L
     return L
+
+
+def device_allocations():
+    """Device allocations the library has made in this process."""
+    return int(lib().omc_device_allocations())
 
 
 def _check(rc, eng=None):
@@ -158,10 +168,12 @@ class Tables:
         self.h = h
 
     @classmethod
-    def from_assets(cls, media, root=None):
+    def from_assets(cls, media, root=None, data="data"):
+        """Tables from the staged assets; `data` names the data folder under
+        the assets root (`data_spin`: the synthetic spin file's variant)."""
         from . import assets
         root = Path(root) if root else assets.require_assets()
-        return cls(root / "pegs4" / "521icru.pegs4dat", root / "pegs4" / "pgs4form.dat", root / "data", media)
+        return cls(root / "pegs4" / "521icru.pegs4dat", root / "pegs4" / "pgs4form.dat", root / data, media)
 
     def get(self, name):
         L = lib()
@@ -400,6 +412,25 @@ class Engine:
                                     _p(nc, _ip), _p(hn, _dp)), self.h)
         return us, irn, idc, nc, hn
 
+    KAT = dict(compton=0, photo=1, pair=2, rayleigh=3, moller=4, bhabha=5, brems=6, annih=7, rannih=8, msdist=9)
+
+    def kat(self, which, q, rn, rn_off, extra=None):
+        """One FP64 sampler per case on scripted streams (omc_kat): returns
+        out[n, 4, 11], nout, used, flags."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        n = len(q)
+        rn = np.ascontiguousarray(rn, dtype=np.float64)
+        off = np.ascontiguousarray(rn_off, dtype=np.int64)
+        ex = None if extra is None else np.ascontiguousarray(extra, dtype=np.float64)
+        out = np.zeros((n, 4, 11))
+        nout = np.zeros(n, dtype=np.int32)
+        used = np.zeros(n, dtype=np.int64)
+        flags = np.zeros(n, dtype=np.uint32)
+        _check(lib().omc_kat(self.h, self.KAT[which] if isinstance(which, str) else int(which), _p(q, _dp),
+                             None if ex is None else _p(ex, _dp), n, _p(rn, _dp), _p(off, _lp), _p(out, _dp),
+                             _p(nout, _ip), _p(used, _lp), _p(flags, _up)), self.h)
+        return out, nout, used, flags
+
     def replay(self, prim, rn, rn_off, dep_cap=2048):
         """FP64 histories on recorded uniform streams; per-history deposits."""
         prim = np.ascontiguousarray(prim, dtype=np.float64)
@@ -494,6 +525,29 @@ class Server:
 
     def release(self, rid):
         _check(lib().omc_server_release(self.h, int(rid)), self.engine.h)
+
+    def completed(self, cap=4096):
+        """Ids of the requests finished since the previous call, in order."""
+        ids = np.zeros(cap, dtype=np.int32)
+        n = C.c_int()
+        _check(lib().omc_server_completed(self.h, _p(ids, _ip), int(cap), C.byref(n)), self.engine.h)
+        return ids[:n.value].tolist()
+
+    def stats(self):
+        """Cycles, drains, kernel launches and finished requests so far."""
+        out = np.zeros(4)
+        _check(lib().omc_server_stats(self.h, _p(out, _dp), 4), self.engine.h)
+        return dict(cycles=int(out[0]), drains=int(out[1]), launches=int(out[2]), finished=int(out[3]))
+
+    def timer_start(self):
+        """Mark the start of a device-timed span on the server's stream."""
+        _check(lib().omc_server_timer(self.h, 0, None), self.engine.h)
+
+    def timer_stop(self):
+        """Device milliseconds since timer_start (waits for the stream)."""
+        ms = C.c_double()
+        _check(lib().omc_server_timer(self.h, 1, C.byref(ms)), self.engine.h)
+        return ms.value
 
     def close(self):
         if getattr(self, "h", None):

@@ -10,12 +10,42 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "mex.h"
 
 static jmp_buf g_jmp;
 static char g_err[512];
 static int g_quiet = 1;
+
+/* Timing of the reference's beamlet loop: with hm_timing(1) the entry runs
+ * with mcOpt.verbose = 2, which makes it create a waitbar before its
+ * beamlet loop, update it after every batch and every beamlet and close it
+ * after the loop (omc_matrad.c:1527-1530, 1594-1600, 1704-1712, 1720-1724);
+ * the shim records the time and progress value of each of those calls. */
+static int g_timing = 0;
+#define WB_CAP 65536
+static double g_wb_t[WB_CAP], g_wb_p[WB_CAP];
+static int g_nwb = 0;
+
+static double mono_s(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+void hm_timing(int on) { g_timing = on; }
+
+/* Waitbar calls of the last hm_dij: time (s, monotonic) and progress
+ * (-1 for the create and close calls); returns how many were recorded. */
+int hm_waitbar_log(double *t, double *p, int cap) {
+    int n = g_nwb < cap ? g_nwb : cap;
+    for (int i = 0; i < n; i++) {
+        t[i] = g_wb_t[i];
+        p[i] = g_wb_p[i];
+    }
+    return n;
+}
 
 /* ----------------------------------------------------------- mx arrays */
 static mxArray *mk(int cls) {
@@ -194,6 +224,17 @@ int mexCallMATLAB(int nlhs, mxArray *plhs[], int nrhs, mxArray *prhs[], const ch
         plhs[0] = mxCreateString(buf);
         return 0;
     }
+    if (g_timing && (!strcmp(name, "waitbar") || !strcmp(name, "close"))) {
+        if (g_nwb < WB_CAP) {
+            int upd = !strcmp(name, "waitbar") && nlhs == 0 && nrhs >= 1 && prhs[0] && prhs[0]->pr;
+            g_wb_t[g_nwb] = mono_s();
+            g_wb_p[g_nwb] = upd ? prhs[0]->pr[0] : -1.0;
+            g_nwb++;
+        }
+        /* the create call's handle is destroyed by the caller after close */
+        if (nlhs >= 1) plhs[0] = mxCreateDoubleScalar(1.0);
+        return 0;
+    }
     if (nlhs >= 1) plhs[0] = NULL;
     return 0;
 }
@@ -251,7 +292,8 @@ long hm_dij(int nx, int ny, int nz, const double *rho, const int32_t *matix, int
     free(tmp);
     mxArray *opt = mk_struct(20);
     double zero = 0, one = 1, seeds[2] = {seed1, seed2};
-    set_field(opt, "verbose", mk_double(&zero, 1, 1, 0));
+    double verb = g_timing ? 2.0 : 0.0;
+    set_field(opt, "verbose", mk_double(&verb, 1, 1, 0));
     set_field(opt, "nHistories", mk_double(&nhist, 1, 1, 0));
     set_field(opt, "nBatches", mk_double(&nbatch, 1, 1, 0));
     set_field(opt, "nSplit", mk_double(&one, 1, 1, 0));
@@ -271,6 +313,7 @@ long hm_dij(int nx, int ny, int nz, const double *rho, const int32_t *matix, int
     mxArray *out[2] = {NULL, NULL};
     long nnz = -1;
     g_err[0] = 0;
+    g_nwb = 0;
     if (setjmp(g_jmp) == 0) {
         mexFunction(2, out, 5, in);
         nnz = (long)out[0]->jc[nbix];

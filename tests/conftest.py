@@ -58,10 +58,15 @@ def engine_for(assets_root):
     """Engine (FP64 + FP32 tables resident) for a named golden case."""
     from ompmc_b200.engine import Engine, Tables
 
-    def get(name, **kw):
-        key = (name, tuple(sorted(kw.items())))
+    def get(name, data="data", **kw):
+        """data: the data folder under the assets root (`data_spin`: the
+        synthetic, non-constant spin file)."""
+        key = (name, data, tuple(sorted(kw.items())))
         if key not in _engines:
-            t = Tables.from_assets(CASES[name]["media"], assets_root)
+            if data == "data_spin":
+                from ompmc_b200 import assets as A
+                A.stage_spin_variant(assets_root)
+            t = Tables.from_assets(CASES[name]["media"], assets_root, data=data)
             _engines[key] = Engine(t, case_phantom(name), **kw)
         return _engines[key]
     yield get

@@ -11,6 +11,13 @@ Fixtures (all seeded; reference RNG seeds 97 33, one thread):
                       (stored exactly as integers rn * 2^24, RANMAR's
                       resolution) and its deposit sequence (region, energy)
   replaysplit_<case>.npz  the same with photon splitting, nsplit = 20
+  replayspin_<case>.npz   the same with the synthetic, non-constant spin file
+                      (assets.write_spin_synthetic; data folder data_spin)
+  kat_<case>.npz      known answers of every interaction sampler and of
+                      msdist: seeded particles in random voxels, scripted
+                      streams, the reference's output particles and
+                      random-number counts (katspin_: with the synthetic spin
+                      file, which the MS sampler inside msdist reads)
   dose*_<case>.npz    reference CLI dose and relative uncertainty of the
                       voxels above 5 % of the maximum (8 threads, 50 batches;
                       sources in DOSE: 6 MV and 18 MV photon spectra, 6 MeV
@@ -56,8 +63,9 @@ TABLES = ["ge0", "ge1", "gmfp0", "gmfp1", "gbr10", "gbr11", "gbr20", "gbr21", "c
           "psig_e", "xcc", "blcc", "expeke1", "spin_rej", "ums", "fms", "wms", "ims", "meke"]
 
 
-def case_inp(name, ncase=100000, nbatch=10, nsplit=1):
-    """Phantom + spectrum + `.inp` of a case under assets/golden_work."""
+def case_inp(name, ncase=100000, nbatch=10, nsplit=1, spin=False):
+    """Phantom + spectrum + `.inp` of a case under assets/golden_work.
+    spin: the data folder with the synthetic (non-constant) spin file."""
     A.require_assets()
     c = CASES[name]
     ph = c["phantom"]()
@@ -66,7 +74,11 @@ def case_inp(name, ncase=100000, nbatch=10, nsplit=1):
         A.write_egsphant(pf, ph)
     run = A.default_run(pf, ncase=ncase, nbatch=nbatch, collimator=c["collimator"])
     run.nsplit = nsplit
+    if spin:
+        run.data_folder = str(A.stage_spin_variant()) + "/"
     base = WORK / (f"{name}_{ncase}" if nsplit == 1 else f"{name}_{ncase}_split{nsplit}")
+    if spin:
+        base = base.with_name(base.name + "_spin")
     A.write_inp(base, run)
     return base, ph
 
@@ -117,9 +129,9 @@ def _rays(name, out):
     np.savez_compressed(out, rays=rays, ustep=us, irnew=irn, idisc=idc, ncalls=nc, hownear=hn, cap=cap)
 
 
-def _replay(name, out):
+def _replay(name, out, spin=False):
     from oracle.ref import Reference
-    base, _ = case_inp(name)
+    base, _ = case_inp(name, spin=spin)
     r = Reference.open(base)
     nh = {"water30": 200, "slab64": 150, "ctsmall": 150}[name]
     res = r.run(nh)
@@ -143,14 +155,120 @@ def _replaysplit(name, out):
                         dep_e=res["dep_e"], d_off=res["d_off"], nsplit=SPLIT)
 
 
-def _tables(name, out):
+def _replayspin(name, out):
+    """As _replay, with the synthetic spin file (spin rejection and the MS
+    moment corrections active)."""
+    _replay(name, out, spin=True)
+
+
+def _tables(name, out, spin=False):
     from oracle.ref import Reference
-    base, _ = case_inp(name)
+    base, _ = case_inp(name, spin=spin)
     r = Reference.open(base)
     d = {n: r.table(n) for n in TABLES}
     for k, v in r.spin_scalars().items():
         d["s_" + k] = np.array(v)
     np.savez_compressed(out, **d)
+
+
+def _tablesspin(name, out):
+    _tables(name, out, spin=True)
+
+
+KAT_CASES = 120        # cases per sampler
+KAT_STREAM = 4096      # uniforms offered per case (multiples of 2^-24)
+RM = 0.5109989461
+
+
+def kat_inputs(ph, which, n, rng):
+    """Particles (x,y,z,u,v,w,e,wt,ir,iq,dnear; e total energy) for the
+    sampler `which` (oracle.ref.Reference.SAMPLERS order, 9 = msdist) in
+    random voxels of the phantom, and (de, tustep) for msdist."""
+    nx, ny, nz = ph.shape
+    i, j, k = rng.integers(0, nx, n), rng.integers(0, ny, n), rng.integers(0, nz, n)
+    fx, fy, fz = rng.random((3, n))
+    x = ph.xb[i] + fx * (ph.xb[i + 1] - ph.xb[i])
+    y = ph.yb[j] + fy * (ph.yb[j + 1] - ph.yb[j])
+    z = ph.zb[k] + fz * (ph.zb[k + 1] - ph.zb[k])
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    ir = 1 + i + j * nx + k * nx * ny
+    logu = lambda lo, hi: np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+    iq = np.zeros(n)
+    if which == 0:
+        e = logu(0.02, 18.0)                    # compton
+    elif which == 1:
+        e = logu(0.01, 1.0)                     # photo
+    elif which == 2:
+        e = logu(1.03, 18.0)                    # pair
+    elif which == 3:
+        e = logu(0.01, 2.0)                     # rayleigh
+    elif which in (4, 6, 9):
+        iq = -np.ones(n) if which == 4 else rng.choice([-1.0, 1.0], n)
+        e = logu(0.05, 18.0) + RM               # moller, brems, msdist
+    elif which in (5, 7):
+        iq = np.ones(n)
+        e = logu(0.05 if which == 5 else 0.01, 18.0) + RM   # bhabha, annih in flight
+    else:
+        iq = np.ones(n)
+        e = np.full(n, RM)                      # rannih: at rest
+    q = np.column_stack([x, y, z, d, e, np.ones(n), ir, iq, np.zeros(n)]).astype(np.float64)
+    extra = None
+    if which == 9:
+        eke = e - RM
+        rhof = ph.rho.ravel()[ir - 1]
+        tustep = 10.0 ** rng.uniform(-3.5, -1.0, n) * eke / np.maximum(rhof, 1e-3)
+        de = np.minimum(tustep * np.maximum(rhof, 1e-3) * 2.0 * rng.uniform(0.5, 1.5, n), 0.5 * eke)
+        extra = np.column_stack([de, tustep])
+    return q, extra
+
+
+def _kat(name, out, spin=False):
+    """Every interaction sampler and msdist on seeded particles and scripted
+    streams: the reference's outputs and random-number counts."""
+    from oracle.ref import Reference
+    base, ph = case_inp(name, spin=spin)
+    r = Reference.open(base)
+    rng = np.random.default_rng(4711 + (1 if spin else 0))
+    names = {v: k for k, v in Reference.SAMPLERS.items()}
+    res = {}
+    for which in range(10):
+        q, extra = kat_inputs(ph, which, KAT_CASES, rng)
+        streams, outs, nouts, used = [], [], [], []
+        for c in range(KAT_CASES):
+            rn_int = rng.integers(0, 1 << 24, KAT_STREAM, dtype=np.uint32)
+            rn = rn_int.astype(np.float64) / 16777216.0
+            o = np.zeros((4, 11))
+            if which == 9:
+                ustep, u, fin = r.msdist(q[c], extra[c, 0], extra[c, 1], rn)
+                o[0, 0] = ustep
+                o[0, 1:7] = fin
+                nout = 1
+            else:
+                u, parts = r.sampler(names[which], q[c], rn)
+                nout = len(parts)
+                o[:nout] = parts
+            if u < 0:
+                raise RuntimeError(f"stream of {KAT_STREAM} numbers too short for sampler {which}")
+            streams.append(rn_int[:u])
+            outs.append(o)
+            nouts.append(nout)
+            used.append(u)
+        off = np.concatenate([[0], np.cumsum([len(x) for x in streams])]).astype(np.int64)
+        key = "msdist" if which == 9 else names[which]
+        res[f"{key}_q"] = q
+        if extra is not None:
+            res[f"{key}_extra"] = extra
+        res[f"{key}_rn_int"] = np.concatenate(streams).astype(np.uint32)
+        res[f"{key}_rn_off"] = off
+        res[f"{key}_out"] = np.array(outs)
+        res[f"{key}_nout"] = np.array(nouts, dtype=np.int32)
+        res[f"{key}_used"] = np.array(used, dtype=np.int64)
+    np.savez_compressed(out, **res)
+
+
+def _katspin(name, out):
+    _kat(name, out, spin=True)
 
 
 # Dose fixtures: name -> (case, spectrum or None, mono energy MeV, charge, histories)
@@ -164,7 +282,13 @@ DOSE = {
     # photon splitting, nsplit = SPLIT (6th field)
     "dosesplit_water30": ("water30", "6mv", 1.25, 0, 1_000_000, SPLIT),
     "dosesplit_slab64": ("slab64", "6mv", 1.25, 0, 1_000_000, SPLIT),
+    # the synthetic spin file (7th field): spin rejection and MS moment
+    # corrections active; electrons of 6 MeV make the multiple scattering
+    # the dominant physics
+    "dosespin_slab64": ("slab64", "6mv", 1.25, 0, 2_000_000, 1, True),
+    "doseespin_water30": ("water30", None, 6.0, -1, 1_000_000, 1, True),
 }
+SPIN_CASES = ["water30", "slab64", "ctsmall"]
 
 
 def make_dose(fixture, nbatch=50, cores=8):
@@ -172,6 +296,7 @@ def make_dose(fixture, nbatch=50, cores=8):
     from oracle.ref import run_cli
     name, spectrum, mono, charge, ncase = DOSE[fixture][:5]
     nsplit = DOSE[fixture][5] if len(DOSE[fixture]) > 5 else 1
+    spin = DOSE[fixture][6] if len(DOSE[fixture]) > 6 else False
     A.require_assets()
     c = CASES[name]
     ph = c["phantom"]()
@@ -181,6 +306,8 @@ def make_dose(fixture, nbatch=50, cores=8):
     run = A.default_run(pf, spectrum=spectrum, ncase=ncase, nbatch=nbatch, collimator=c["collimator"],
                         mono_energy=mono, charge=charge)
     run.nsplit = nsplit
+    if spin:
+        run.data_folder = str(A.stage_spin_variant()) + "/"
     base = WORK / f"{fixture}_{ncase}"
     A.write_inp(base, run)
     loop_s, _ = run_cli(base, f"golden_{fixture}", cores=cores)
@@ -189,7 +316,8 @@ def make_dose(fixture, nbatch=50, cores=8):
     np.savez_compressed(HERE / f"{fixture}.npz", idx=keep.astype(np.int32), dose=dose.ravel()[keep],
                         unc=unc.ravel()[keep].astype(np.float32), shape=np.array(dose.shape), dmax=dose.max(),
                         ncase=ncase, nbatch=nbatch, loop_seconds=loop_s, cores=cores,
-                        spectrum=str(spectrum or ""), mono_energy=mono, charge=charge, nsplit=nsplit)
+                        spectrum=str(spectrum or ""), mono_energy=mono, charge=charge, nsplit=nsplit,
+                        spin_data="data_spin" if spin else "data")
 
 
 GAMMA_HIST = {"water30": 100_000_000, "slab64": 400_000_000}
@@ -206,6 +334,39 @@ def make_gamma(name, nbatch=100, cores=8):
     np.savez_compressed(HERE / f"gamma_{name}.npz", idx=keep.astype(np.int32), dose=dose.ravel()[keep],
                         unc=unc.ravel()[keep].astype(np.float32), shape=np.array(dose.shape), dmax=dose.max(),
                         ncase=ncase, nbatch=nbatch, loop_seconds=loop_s, cores=cores)
+
+
+# Full-size CT-like phantoms of the benchmark workloads: name -> (phantom,
+# spectrum, histories, batches).  One reference CLI run each serves the
+# z-test (its batch uncertainty) and the gamma test (its dose); the fixture
+# keeps the voxels above 10 % of the maximum, dose as float32.
+BIG = {
+    # 128x128x96 x 0.3 cm, one 10x10 cm2 6 MV-like beam
+    "ct128": (lambda: A.ct_phantom(128, 128, 96, 0.3, seed=1234), "6mv", 250_000_000, 50),
+    # 256x256x160 x 0.2 cm, one 10x10 cm2 18 MV-like beam (pair/triplet production)
+    "ct256": (A.ct_phantom_large, "18mv", 120_000_000, 40),
+}
+
+
+def make_big(name, cores=8):
+    """Reference CLI dose of a BIG case -> refbig_<name>.npz."""
+    from oracle.ref import run_cli
+    mk, spectrum, ncase, nbatch = BIG[name]
+    A.require_assets()
+    ph = mk()
+    pf = WORK / f"{name}.egsphant"
+    if not pf.exists():
+        A.write_egsphant(pf, ph)
+    run = A.default_run(pf, spectrum=spectrum, ncase=ncase, nbatch=nbatch, collimator=(-5, 5, -5, 5))
+    base = WORK / f"refbig_{name}_{ncase}"
+    A.write_inp(base, run)
+    loop_s, _ = run_cli(base, f"refbig_{name}", cores=cores, timeout=12 * 3600)
+    dose, unc, _ = A.read_3ddose(A.ASSETS / "out" / f"refbig_{name}.3ddose")
+    keep = np.flatnonzero(dose.ravel() > 0.1 * dose.max())
+    np.savez_compressed(HERE / f"refbig_{name}.npz", idx=keep.astype(np.int32),
+                        dose=dose.ravel()[keep].astype(np.float32), unc=unc.ravel()[keep].astype(np.float32),
+                        shape=np.array(dose.shape), dmax=dose.max(), ncase=ncase, nbatch=nbatch,
+                        loop_seconds=loop_s, cores=cores, spectrum=spectrum, collimator=np.array([-5, 5, -5, 5.0]))
 
 
 DIJ = dict(gantry=[0.0, 90.0], bixel=1.0, field=(2.0, 2.0), nhist=100000, nbatch=10, rel=1e-4)
@@ -241,12 +402,15 @@ def make_dij(gaussian=False):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", default=None)
+    ap.add_argument("--cores", type=int, default=8, help="host cores of the refbig_* reference runs")
     a = ap.parse_args()
     from oracle.ref import build
     build()
     A.require_assets()
     WORK.mkdir(parents=True, exist_ok=True)
     jobs = [("rays", n) for n in CASES] + [("replay", n) for n in CASES] + [("replaysplit", n) for n in CASES]
+    jobs += [("replayspin", n) for n in SPIN_CASES]
+    jobs += [("kat", "slab64"), ("kat", "ctsmall"), ("katspin", "slab64")]
     for what, name in jobs:
         fn = f"{what}_{name}"
         if a.only and a.only not in fn:
@@ -263,6 +427,11 @@ def main():
             continue
         print("generating gamma reference", name, flush=True)
         make_gamma(name)
+    for name in BIG:
+        if a.only and a.only not in f"refbig_{name}":
+            continue
+        print("generating refbig", name, flush=True)
+        make_big(name, cores=a.cores)
     if not a.only or a.only in "dij_ctsmall":
         print("generating dij_ctsmall", flush=True)
         make_dij()

@@ -101,3 +101,36 @@ def test_commented_key_counts_as_missing(tmp_path, assets_root):
     p = subprocess.run([str(CLI_PATH), "-i", str(tmp_path / "c"), "-o", "out"], capture_output=True, text=True,
                        timeout=120)
     assert p.returncode != 0 and "Can not find 'ncase' key on input file." in p.stdout + p.stderr
+
+
+def test_sampler_fixtures_reproduce_from_the_oracle(tmp_path):
+    """The sampler known answers (tests/golden/kat_slab64.npz) come out of the
+    live oracle again, bit for bit, for the first cases of every sampler."""
+    import subprocess
+    import sys
+    from tests.conftest import GOLDEN, REPO
+    code = (f"import sys, numpy as np; sys.path.insert(0, {str(REPO)!r}); "
+            "from tests.golden import make_golden as M; from oracle.ref import Reference; "
+            "M.WORK.mkdir(parents=True, exist_ok=True); "
+            "base, ph = M.case_inp('slab64'); r = Reference.open(base); "
+            f"g = dict(np.load({str(GOLDEN / 'kat_slab64.npz')!r})); bad = 0; "
+            "names = {v: k for k, v in Reference.SAMPLERS.items()}\n"
+            "for w in range(10):\n"
+            "    key = 'msdist' if w == 9 else names[w]\n"
+            "    rn = g[key + '_rn_int'].astype(np.float64) / 16777216.0; off = g[key + '_rn_off']\n"
+            "    for c in range(5):\n"
+            "        s = rn[off[c]:off[c + 1]]\n"
+            "        if w == 9:\n"
+            "            us, u, fin = r.msdist(g[key + '_q'][c], *g[key + '_extra'][c], s)\n"
+            "            ok = u == g[key + '_used'][c] and us == g[key + '_out'][c, 0, 0] and "
+            "np.array_equal(fin, g[key + '_out'][c, 0, 1:7])\n"
+            "        else:\n"
+            "            u, parts = r.sampler(key, g[key + '_q'][c], s)\n"
+            "            ok = u == g[key + '_used'][c] and np.array_equal(parts, g[key + '_out'][c, :len(parts)])\n"
+            "        bad += not ok\n"
+            "print('BAD', bad)\n")
+    from oracle import ref
+    ref.build()
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert "BAD 0" in p.stdout, p.stdout[-500:]

@@ -131,3 +131,50 @@ def test_beam_request_matches_run_beam_statistically(engine_for, assets_root):
     z = (d1[m] - d0[m]) / np.sqrt((u1[m] * d1[m]) ** 2 + (u0[m] * d0[m]) ** 2)
     assert np.mean(np.abs(z) < 3) >= 0.99
     assert abs(z.mean()) < 0.25
+
+
+def test_submissions_from_two_threads_while_a_third_steps(engine_for, assets_root):
+    """Two producer threads submit beamlet requests while the main thread
+    steps the server (omc_server_* serialise on the server's mutex).  Every
+    request's column equals the one it gets submitted from one thread: a
+    request's streams depend only on its seed, not on its id or timing."""
+    import threading
+    from ompmc_b200.engine import Server, load_spectrum
+    eng = engine_for("ctsmall")
+    bl = bixels(engine_for)
+    bl["spectrum"] = load_spectrum(assets_root / "spectra" / "6mv.spectrum")
+    jobs = [(i % 16, 8000 + 1000 * i, 500 + i) for i in range(12)]      # (bixel, histories, seed)
+    one = Server(eng, seed=2)
+    bs1 = one.beamlet_set(bl)
+    ref = run_all(one, {k: one.submit_beamlet(bs1, b, n, 10, 1e-4, seed=sd) for k, (b, n, sd) in enumerate(jobs)})
+    one.close()
+    srv = Server(eng, seed=3)
+    bs = srv.beamlet_set(bl)
+    ids, errors = {}, []
+    lock = threading.Lock()
+
+    def produce(part):
+        try:
+            for k in part:
+                b, n, sd = jobs[k]
+                rid = srv.submit_beamlet(bs, b, n, 10, 1e-4, seed=sd)
+                with lock:
+                    ids[k] = rid
+        except Exception as ex:           # reported by the main thread
+            errors.append(ex)
+
+    threads = [threading.Thread(target=produce, args=(range(p, len(jobs), 2),)) for p in range(2)]
+    for t in threads:
+        t.start()
+    while any(t.is_alive() for t in threads) or srv.step(4) > 0:
+        srv.step(2)
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    assert sorted(ids) == list(range(len(jobs)))
+    assert len(set(ids.values())) == len(jobs)
+    got = run_all(srv, ids)
+    srv.close()
+    for k in range(len(jobs)):
+        assert np.array_equal(got[k][0], ref[k][0])
+        np.testing.assert_allclose(got[k][1], ref[k][1], rtol=1e-9)

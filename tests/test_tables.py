@@ -18,13 +18,14 @@ from tests.conftest import CASES, REPO
 pytestmark = pytest.mark.filterwarnings("ignore::RuntimeWarning")
 
 
-def reference_tables(case, tmp_path):
+def reference_tables(case, tmp_path, spin=False):
     from oracle import ref
     ref.build()
     out = tmp_path / f"ref_{case}.npz"
+    what = "_tablesspin" if spin else "_tables"
     code = (f"import sys; sys.path.insert(0, {str(REPO)!r}); "
             f"from tests.golden import make_golden as M; M.WORK.mkdir(parents=True, exist_ok=True); "
-            f"M._tables({case!r}, {str(out)!r})")
+            f"M.{what}({case!r}, {str(out)!r})")
     p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
     assert p.returncode == 0, p.stderr[-2000:]
     return dict(np.load(out))
@@ -49,13 +50,24 @@ def etap_exact_bins(tables, nmed):
     return ok
 
 
-@pytest.mark.parametrize("case", list(CASES))
-def test_tables_match_reference(case, tmp_path, assets_root):
+@pytest.mark.parametrize("case,spin", [(c, False) for c in CASES] + [("slab64", True), ("ctsmall", True)])
+def test_tables_match_reference(case, spin, tmp_path, assets_root):
+    """spin: the data folder with the synthetic, non-constant spin file, whose
+    rejection surface and moment corrections differ from 1."""
+    from ompmc_b200 import assets as A
     from ompmc_b200.engine import Tables
-    ref = reference_tables(case, tmp_path)
+    if spin:
+        A.stage_spin_variant(assets_root)
+    ref = reference_tables(case, tmp_path, spin)
     media = CASES[case]["media"]
     nmed = len(media)
-    t = Tables.from_assets(media, assets_root)
+    t = Tables.from_assets(media, assets_root, data="data_spin" if spin else "data")
+    if spin:
+        # the variant really differs from the neutral file
+        sr = t.get("spin_rej")
+        assert sr.min() < 0.5 and sr.max() == 1.0
+        q1 = t.get("q1ce_ms0")
+        assert np.any(np.abs(q1[q1 != 0] - 1.0) > 0.01)
     ok_etap = etap_exact_bins(t, nmed)
     bad = []
     for name, a in ref.items():

@@ -30,9 +30,15 @@ def test_noalloc_matches_run_beam_twice(engine_for, assets_root):
     coll = CASES["water30"]["collimator"]
     d0, u0, s0 = eng.run_beam(100000, 10, seed=4242, mode=PLAIN_FP64, spectrum=spec, collimator=coll)
     assert s0["flags"] == 0 and d0.max() > 0
-    for _ in range(2):
+    from ompmc_b200.engine import device_allocations
+    for k in range(2):
+        before = device_allocations()
         d, u, s = eng.run_beam_noalloc(100000, 10, seed=4242, spectrum=spec, collimator=coll)
+        if k == 1:
+            # after the warm-up call, a call makes no device allocation
+            assert device_allocations() == before
         assert s["flags"] == 0
+        assert s["launches"] == s0["launches"]
         assert s["histories"] == s0["histories"]
         np.testing.assert_allclose(d, d0, rtol=1e-9, atol=1e-30)
         m = d0 > 0
