@@ -74,6 +74,9 @@ typedef struct {
 /* ------------------------------------------------------------ engine */
 #define OMC_PLAIN_FP64 0   /* history-based, one thread per history, FP64 */
 #define OMC_EVENT_FP32 1   /* event-based queues, FP32 transport, FP64 tallies */
+#define OMC_EVENT_FP64 2   /* the same event-based form with FP64 transport
+                              (omc_run_beam only; no photon splitting):
+                              separates the event form's gain from FP32's */
 #define OMC_MAX_NSPLIT 64  /* largest photon splitting factor (omc_options.nsplit) */
 
 typedef struct {
@@ -312,6 +315,14 @@ int omc_server_timer(omc_server *s, int stop, double *ms);
  * by one with events around each kernel, and omc_profile_last reports the
  * per-kernel times and transport counters of everything it has run. */
 int omc_server_stats(omc_server *s, double *out, int n);
+/* Tail budget of a server's requests (no reference counterpart): once a
+ * request's histories are all injected and at most tail_particles (default
+ * 4096) of its particles are left, its electrons get tail_boost (default:
+ * the engine's tail_boost option) times the cycle's budget of tstep-loop
+ * iterations per event, so its longest chains finish in fewer cycles.
+ * tail_particles 0 turns it off; a negative value, or tail_boost <= 0,
+ * keeps the current value.  Results do not depend on it. */
+int omc_server_params(omc_server *s, int64_t tail_particles, int tail_boost);
 
 /* ---------------------------------------------- drop-in CLI (dosxyz)
  * The whole omc_dosxyz program (omc_dosxyz.c:1072-1307): reads

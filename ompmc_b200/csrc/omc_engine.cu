@@ -634,7 +634,8 @@ int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, ui
                  double *unc, double *stats) {
     if (!e || !b) return global_err(OMC_E_ARG, "omc_run_beam: null argument");
     if (nbatch < 2) return set_err(e, OMC_E_ARG, "nbatch must be >= 2 for the batch uncertainty");
-    if (mode != OMC_PLAIN_FP64 && mode != OMC_EVENT_FP32) return set_err(e, OMC_E_ARG, "unknown mode");
+    if (mode != OMC_PLAIN_FP64 && mode != OMC_EVENT_FP32 && mode != OMC_EVENT_FP64)
+        return set_err(e, OMC_E_ARG, "unknown mode");
     if (b->energy.n > 0 && (!b->energy.cdf1 || !b->energy.cdf2)) return set_err(e, OMC_E_ARG, "spectrum arrays missing");
     if (b->energy.charge < -1 || b->energy.charge > 1) return set_err(e, OMC_E_ARG, "charge must be -1, 0 or 1");
     cudaSetDevice(e->device);
@@ -689,7 +690,8 @@ int omc_run_beam(omc_engine *e, const omc_beam *b, int64_t ncase, int nbatch, ui
         cudaEventDestroy(t0);
         cudaEventDestroy(t1);
     } else {
-        if ((rc = event_run_beam(e, b, nper, nbatch, seed, sum.as<double>(), sum2.as<double>(), acc.as<double>() + 1,
+        auto run = mode == OMC_EVENT_FP64 ? event_run_beam<double> : event_run_beam<float>;
+        if ((rc = run(e, b, nper, nbatch, seed, sum.as<double>(), sum2.as<double>(), acc.as<double>() + 1,
                                  ks)))
             return rc;
     }

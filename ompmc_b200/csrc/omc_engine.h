@@ -67,11 +67,14 @@ struct KernelStats {
 }  // namespace omc
 
 namespace omc {
-struct EventState;
+template <typename R>
+struct EventStateT;
+using EventState = EventStateT<float>;
 }
 
 struct omc_engine {
     omc::EventState *ev = nullptr;  // event-form queues (allocated on first use)
+    omc::EventStateT<double> *ev64 = nullptr;  // the FP64 event form's (allocated on first use)
     omc::Tables tabs;
     omc::Phantom ph;
     omc::Regions reg;

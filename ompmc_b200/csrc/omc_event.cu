@@ -29,6 +29,8 @@
 #include <cstdio>
 
 #include "omc_event.h"
+
+
 #include "omc_rng.cuh"
 #include "omc_source.cuh"
 
@@ -38,9 +40,20 @@ constexpr int EV_BUDGET = 200000;  // transport steps one event may take
 constexpr int EV_MAXOUT = 1;       // secondaries an event emits: every interaction sampler pushes one
 constexpr int EV_MAXOUT_SPLIT = 2; // products of a split photon's sub-photon (pair: two)
 constexpr int EV_MAX_BLOCK = 256;  // launch bound of the transport kernels
+// Resident 256-thread blocks per SM the electron kernel is compiled for:
+// four (64 registers) in FP32, two (128 registers) in FP64.  Measured on the
+// served beamlet load and the slab beam: 4 blocks 27.5 and 45.9 M hist/s,
+// 6 blocks 27.3 and 46.1, 8 blocks (32 registers) 27.0 and 45.9, while the
+// 8-block build's spilled frames made 6x the DRAM writes of the 4-block one.
+template <typename R>
+constexpr int electron_minb() {
+    return sizeof(R) == 4 ? 4 : 2;
+}
 
-using TransportKernel = void (*)(DevData<float>, Queue, Queue, Queue, double *, long, Ctl *, uint32_t, int *, int,
-                                 Queue);
+template <typename R>
+using TransportKernelT = void (*)(DevData<R>, QueueT<R>, QueueT<R>, QueueT<R>, double *, long, Ctl *, uint32_t,
+                                  ServeDev *, int, QueueT<R>);
+using TransportKernel = TransportKernelT<float>;
 
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
@@ -48,22 +61,22 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
-template <int MAXOUT>
+template <int MAXOUT, typename R = float>
 struct EvEnv {
-    Philox<float> rng;
+    Philox<R> rng;
     double *tally;
     int pend_ir;
     double pend_e;
-    Part<float> out[MAXOUT];
+    Part<R> out[MAXOUT];
     uint32_t out_pos[MAXOUT];     // parent's stream position at each push
     int nout;
     unsigned flags;
     int work;
     int tleft;                    // tstep-loop iterations left in this event
     int ncross, ndep, natom;
-    __device__ float uni() { return rng.uni(); }
+    __device__ R uni() { return rng.uni(); }
     // Consecutive deposits into one voxel are summed before the atomic.
-    __device__ void deposit(int ir, float e) {
+    __device__ void deposit(int ir, R e) {
         ndep++;
         if (ir != pend_ir) {
             flush();
@@ -73,15 +86,30 @@ struct EvEnv {
     }
     __device__ void flush() {
         if (pend_ir > 0 && pend_e != 0.0) {
-            atomicAdd(&tally[pend_ir - 1], pend_e);
-            natom++;
+            // the lanes of the warp that flush here together into the same
+            // tally element (same voxel and tally slot) add once: the
+            // group's sum, by its lowest lane (+4-5 % on the served beamlet
+            // load and the slab beam over one atomic per lane)
+            double *dst = &tally[pend_ir - 1];
+            const unsigned act = __activemask();
+            const unsigned grp = __match_any_sync(act, (unsigned long long)dst);
+            const int lane = threadIdx.x & 31;
+            double tot = pend_e;
+            if (grp != (1u << lane)) {
+                tot = 0.0;
+                for (unsigned m = grp; m; m &= m - 1) tot += __shfl_sync(grp, pend_e, __ffs(m) - 1);
+            }
+            if (lane == __ffs(grp) - 1) {
+                atomicAdd(dst, tot);
+                natom++;
+            }
         }
         pend_e = 0.0;
         pend_ir = -1;
     }
     __device__ void cross() { ncross++; }
     __device__ bool tstep_take() { return tleft-- > 0; }
-    __device__ bool push(const Part<float> &q) {
+    __device__ bool push(const Part<R> &q) {
         if (nout >= MAXOUT) {
             flags |= ERR_STACK;
             return false;
@@ -100,32 +128,66 @@ struct EvEnv {
     __device__ bool tick() { return ++work < EV_BUDGET; }
 };
 
+template <typename R = float>
 struct SrcEnv {
-    Philox<float> rng;
-    __device__ float uni() { return rng.uni(); }
+    Philox<R> rng;
+    __device__ R uni() { return rng.uni(); }
 };
 
+// A queued particle is read once and written once per event, so its loads
+// and stores bypass L1 and are marked streaming (evict first) in L2, which
+// keeps the caches for the tables, the tallies and the kernels' local frames.
 __device__ __forceinline__ void qload(const Queue &q, int i, Part<float> &p, int &tag, uint32_t &k0, uint32_t &k1,
                                       uint32_t &ctr) {
-    p.x = q.x[i]; p.y = q.y[i]; p.z = q.z[i];
-    p.u = q.u[i]; p.v = q.v[i]; p.w = q.w[i];
-    p.e = q.e[i]; p.wt = q.wt[i];
-    p.ir = q.ir[i];
-    tag = q.tag[i];
+    const float4 a = __ldcs(&q.pos[i]);
+    const float4 b = __ldcs(&q.dir[i]);
+    const uint4 c = __ldcs(&q.id[i]);
+    ctr = __ldcs(&q.ctr[i]);
+    p.x = a.x; p.y = a.y; p.z = a.z; p.u = a.w;
+    p.v = b.x; p.w = b.y; p.e = b.z; p.wt = b.w;
+    p.ir = (int)c.x;
+    tag = (int)c.y;
     p.iq = (tag & 3) - 1;
-    k0 = q.k0[i]; k1 = q.k1[i]; ctr = q.ctr[i];
+    k0 = c.z; k1 = c.w;
+}
+
+__device__ __forceinline__ void qload(const QueueT<double> &q, int i, Part<double> &p, int &tag, uint32_t &k0,
+                                      uint32_t &k1, uint32_t &ctr) {
+    const double2 *pa = (const double2 *)&q.pos[i], *pb = (const double2 *)&q.dir[i];
+    const double2 a0 = __ldcs(pa), a1 = __ldcs(pa + 1), b0 = __ldcs(pb), b1 = __ldcs(pb + 1);
+    const uint4 c = __ldcs(&q.id[i]);
+    ctr = __ldcs(&q.ctr[i]);
+    p.x = a0.x; p.y = a0.y; p.z = a1.x; p.u = a1.y;
+    p.v = b0.x; p.w = b0.y; p.e = b1.x; p.wt = b1.y;
+    p.ir = (int)c.x;
+    tag = (int)c.y;
+    p.iq = (tag & 3) - 1;
+    k0 = c.z; k1 = c.w;
 }
 
 // sp/sr: splitting state, stored where the queue has it (photon queues of
 // splitting engines); -1 = a photon not yet split.
 __device__ __forceinline__ void qstore(const Queue &q, int i, const Part<float> &p, int slot, uint32_t k0, uint32_t k1,
                                        uint32_t ctr, int sp = -1, float sr = 0.f) {
-    q.x[i] = p.x; q.y[i] = p.y; q.z[i] = p.z;
-    q.u[i] = p.u; q.v[i] = p.v; q.w[i] = p.w;
-    q.e[i] = p.e; q.wt[i] = p.wt;
-    q.ir[i] = p.ir;
-    q.tag[i] = (p.iq + 1) | (slot << 2);
-    q.k0[i] = k0; q.k1[i] = k1; q.ctr[i] = ctr;
+    __stcs(&q.pos[i], make_float4(p.x, p.y, p.z, p.u));
+    __stcs(&q.dir[i], make_float4(p.v, p.w, p.e, p.wt));
+    __stcs(&q.id[i], make_uint4((uint32_t)p.ir, (uint32_t)((p.iq + 1) | (slot << 2)), k0, k1));
+    __stcs(&q.ctr[i], ctr);
+    if (q.sp) {
+        q.sp[i] = sp;
+        q.sr[i] = sr;
+    }
+}
+
+__device__ __forceinline__ void qstore(const QueueT<double> &q, int i, const Part<double> &p, int slot, uint32_t k0,
+                                       uint32_t k1, uint32_t ctr, int sp = -1, float sr = 0.f) {
+    double2 *pa = (double2 *)&q.pos[i], *pb = (double2 *)&q.dir[i];
+    __stcs(pa, make_double2(p.x, p.y));
+    __stcs(pa + 1, make_double2(p.z, p.u));
+    __stcs(pb, make_double2(p.v, p.w));
+    __stcs(pb + 1, make_double2(p.e, p.wt));
+    __stcs(&q.id[i], make_uint4((uint32_t)p.ir, (uint32_t)((p.iq + 1) | (slot << 2)), k0, k1));
+    __stcs(&q.ctr[i], ctr);
     if (q.sp) {
         q.sp[i] = sp;
         q.sr[i] = sr;
@@ -135,7 +197,8 @@ __device__ __forceinline__ void qstore(const Queue &q, int i, const Part<float> 
 // Slot of a warp-aggregated append to `q` for the lanes with `want`: from
 // the bottom, or from the top for lanes with `hi`; -1 for the other lanes
 // (or on overflow, flagged).
-__device__ __forceinline__ int warp_append(const Queue &q, bool want, bool hi, unsigned active, unsigned &flags) {
+template <typename Q>
+__device__ __forceinline__ int warp_append(const Q &q, bool want, bool hi, unsigned active, unsigned &flags) {
     const int lane = threadIdx.x & 31;
     const unsigned mlo = __ballot_sync(active, want && !hi);
     const unsigned mhi = __ballot_sync(active, want && hi);
@@ -160,10 +223,12 @@ __device__ __forceinline__ int warp_append(const Queue &q, bool want, bool hi, u
 }
 
 // Entries of a queue (both ends) and the index of the f-th, top end first.
-__device__ __forceinline__ int queue_size(const Queue &q) {
+template <typename Q>
+__device__ __forceinline__ int queue_size(const Q &q) {
     return min(min(*q.count, q.cap) + min(*q.count_hi, q.cap), q.cap);
 }
-__device__ __forceinline__ int queue_index(const Queue &q, int f) {
+template <typename Q>
+__device__ __forceinline__ int queue_index(const Q &q, int f) {
     int nhi = min(*q.count_hi, q.cap);
     return f < nhi ? q.cap - 1 - f : f - nhi;
 }
@@ -176,17 +241,18 @@ __device__ __forceinline__ int queue_index(const Queue &q, int f) {
 // state (sp, sr); secondaries start unsplit.  Photons of zero weight (lost
 // a Russian roulette) would deposit nothing and are not queued.  Returns
 // the particles this lane queued.
-template <int MAXOUT, bool DEFER = false>
-__device__ __forceinline__ int emit(const Queue &outP, const Queue &outE, bool alive, const Part<float> &p,
-                                    EvEnv<MAXOUT> &g, int slot, uint32_t k0, uint32_t k1, float esplit,
-                                    int sp = -1, float sr = 0.f, const Queue *outI = nullptr, bool defer = false) {
+template <int MAXOUT, bool DEFER = false, typename R = float>
+__device__ __forceinline__ int emit(const QueueT<R> &outP, const QueueT<R> &outE, bool alive, const Part<R> &p,
+                                    EvEnv<MAXOUT, R> &g, int slot, uint32_t k0, uint32_t k1, float esplit,
+                                    int sp = -1, float sr = 0.f, const QueueT<R> *outI = nullptr,
+                                    bool defer = false) {
     const unsigned full = 0xffffffffu;
     uint64_t pkey = ((uint64_t)k1 << 32) | k0;
     int queued = 0;
 #pragma unroll
     for (int k = 0; k < 1 + MAXOUT; k++) {
         bool has;
-        Part<float> q;
+        Part<R> q;
         uint32_t a0 = k0, a1 = k1, ac;
         if (k == 0) {
             has = alive;
@@ -206,14 +272,14 @@ __device__ __forceinline__ int emit(const Queue &outP, const Queue &outE, bool a
             g.flags |= ERR_NAN;
             has = false;
         }
-        if (has && q.iq == 0 && q.wt == 0.f) has = false;
+        if (has && q.iq == 0 && q.wt == R(0)) has = false;
         // an electron left at its discrete interaction goes to the
         // interaction queue
         const bool toi = DEFER && k == 0 && defer;
         bool isph = has && q.iq == 0 && !toi;
         bool isel = has && q.iq != 0 && !toi;
         int ip = warp_append(outP, isph, false, full, g.flags);
-        int ie = warp_append(outE, isel, esplit > 0.f && q.e > esplit, full, g.flags);
+        int ie = warp_append(outE, isel, esplit > 0.f && q.e > (R)esplit, full, g.flags);
         if (ip >= 0) qstore(outP, ip, q, slot, a0, a1, ac, k == 0 ? sp : -1, k == 0 ? sr : 0.f);
         if (ie >= 0) qstore(outE, ie, q, slot, a0, a1, ac);
         queued += (ip >= 0) + (ie >= 0);
@@ -260,8 +326,8 @@ __device__ __forceinline__ void add_live(int *live, int nbmax, int slot, int del
 // returns true while it has sub-photons left.  The draws differ from the
 // plain form's order (one stream per ray), the sampled distribution is the
 // same.
-template <typename Env>
-__device__ __forceinline__ bool split_event(const DevData<float> &D, Env &g, Part<float> &p, int &sp, float &sr) {
+template <typename R, typename Env>
+__device__ __forceinline__ bool split_event(const DevData<R> &D, Env &g, Part<R> &p, int &sp, float &sr) {
     const int ns = D.nsplit;
     if (sp < 0) {
         if (p.e <= pcut_of(D, p.ir) || p.wt == 0.f) {
@@ -317,10 +383,10 @@ __device__ __forceinline__ bool split_event(const DevData<float> &D, Env &g, Par
 // D.defer_interact).  `qi`: the interaction queue (EV_ELECTRON with
 // D.defer_interact appends there).
 enum { EV_PHOTON = 0, EV_ELECTRON = 1, EV_SPLIT = 2, EV_INTERACT = 3, EV_ELECTRON_DEFER = 4 };
-template <int KIND>
-__device__ __forceinline__ void transport_events(const DevData<float> &D, const Queue &in, const Queue &outP,
-                                                 const Queue &outE, double *tallies, long nvox, Ctl *ctl,
-                                                 uint32_t seedw, int *live, int nbmax, const Queue &qi) {
+template <int KIND, typename R = float>
+__device__ __forceinline__ void transport_events(const DevData<R> &D, const QueueT<R> &in, const QueueT<R> &outP,
+                                                 const QueueT<R> &outE, double *tallies, long nvox, Ctl *ctl,
+                                                 uint32_t seedw, ServeDev *sd, int nbmax, const QueueT<R> &qi) {
     constexpr int MAXOUT = KIND == EV_SPLIT ? EV_MAXOUT_SPLIT : EV_MAXOUT;
     const unsigned full = 0xffffffffu;
     constexpr bool ELECTRON = KIND == EV_ELECTRON || KIND == EV_ELECTRON_DEFER;
@@ -339,7 +405,7 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
         if (base >= n) break;
         const bool valid = base + lane < n;
         const int i = valid ? queue_index(in, base + lane) : 0;
-        Part<float> p;
+        Part<R> p;
         int tag = 0;
         uint32_t k0 = 0, k1 = 0, pos = 0;
         if (valid) qload(in, i, p, tag, k0, k1, pos);
@@ -350,7 +416,7 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
             sr = in.sr[i];
         }
         const int slot = tag >> 2;
-        EvEnv<MAXOUT> g;
+        EvEnv<MAXOUT, R> g;
         g.rng.init(((uint64_t)k1 << 32) | k0, seedw, pos);
         g.tally = tallies + (long)slot * nvox;
         g.pend_ir = -1;
@@ -358,17 +424,17 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
         g.nout = 0;
         g.flags = 0;
         g.work = 0;
-        g.tleft = tsteps;
+        g.tleft = (sd && valid) ? tsteps * sd->boost[slot / nbmax] : tsteps;
         g.ncross = g.ndep = g.natom = 0;
         bool alive = false, defer = false;
         if (valid) {
             if (KIND == EV_PHOTON) {
                 alive = D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p);
             } else if (ELECTRON) {
-                int r = electron_step<float, EvEnv<MAXOUT>, KIND == EV_ELECTRON_DEFER>(D, g, p);
+                int r = electron_step<R, EvEnv<MAXOUT, R>, KIND == EV_ELECTRON_DEFER>(D, g, p);
                 alive = r != E_DEAD;
                 defer = r == E_INTERACT;
-            } else if (KIND == EV_SPLIT) {
+            } else if constexpr (KIND == EV_SPLIT) {
                 alive = split_event(D, g, p, sp, sr);
             } else {
                 electron_interact(D, g, p);
@@ -377,9 +443,9 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
             g.flush();
         }
         int emitted = KIND == EV_ELECTRON_DEFER
-                          ? emit<MAXOUT, true>(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr, &qi, defer)
-                          : emit(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr);
-        if (live) add_live(live, nbmax, valid ? slot : 0, valid ? emitted - 1 : 0, full);
+                          ? emit<MAXOUT, true, R>(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr, &qi, defer)
+                          : emit<MAXOUT, false, R>(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr);
+        if (sd) add_live(sd->live, nbmax, valid ? slot : 0, valid ? emitted - 1 : 0, full);
         flags |= g.flags;
         c_ev += valid;
         c_steps += g.work;
@@ -397,46 +463,47 @@ __device__ __forceinline__ void transport_events(const DevData<float> &D, const 
 
 // Photon events of the queued photons.  `live` (may be null) receives the
 // change of each serving request's live-particle count.
-__global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_step(DevData<float> D, Queue in, Queue outP, Queue outE,
-                                                     double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
-                                                     int *live, int nbmax, Queue qi) {
-    transport_events<EV_PHOTON>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax, qi);
+template <typename R>
+__global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_step(DevData<R> D, QueueT<R> in, QueueT<R> outP,
+                                                     QueueT<R> outE, double *tallies, long nvox, Ctl *ctl,
+                                                     uint32_t seedw, ServeDev *sd, int nbmax, QueueT<R> qi) {
+    transport_events<EV_PHOTON, R>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd, nbmax, qi);
 }
 
 // Photon events of a splitting engine (nsplit > 1): one sub-photon each.
 __global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_split_step(DevData<float> D, Queue in, Queue outP,
                                                            Queue outE, double *tallies, long nvox, Ctl *ctl,
-                                                           uint32_t seedw, int *live, int nbmax, Queue qi) {
-    transport_events<EV_SPLIT>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax, qi);
+                                                           uint32_t seedw, ServeDev *sd, int nbmax, Queue qi) {
+    transport_events<EV_SPLIT>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd, nbmax, qi);
 }
 
 // Electron/positron events of the queued charged particles: at most the
 // cycle's budget of tstep-loop iterations each, then the particle is
-// re-queued.  The step is latency bound and more resident warps hide more
-// of it: eight blocks of 256 threads per SM (full occupancy, 32 registers
-// with spills to L1-cached local memory) measured 5 % faster than four
-// (64 registers) and 12 % faster than two (114 registers, no spills).
-template <bool DEFER>
-__global__ void __launch_bounds__(EV_MAX_BLOCK, 8) k_electron_step(DevData<float> D, Queue in, Queue outP, Queue outE,
-                                                       double *tallies, long nvox, Ctl *ctl, uint32_t seedw,
-                                                       int *live, int nbmax, Queue qi) {
-    transport_events<DEFER ? EV_ELECTRON_DEFER : EV_ELECTRON>(D, in, outP, outE, tallies, nvox, ctl, seedw, live,
-                                                               nbmax, qi);
+// re-queued.  The step is latency bound; the occupancy it is compiled for
+// (electron_minb) trades resident warps against spilled local frames.
+template <bool DEFER, typename R = float>
+__global__ void __launch_bounds__(EV_MAX_BLOCK, electron_minb<R>())
+    k_electron_step(DevData<R> D, QueueT<R> in, QueueT<R> outP, QueueT<R> outE, double *tallies, long nvox, Ctl *ctl,
+                    uint32_t seedw, ServeDev *sd, int nbmax, QueueT<R> qi) {
+    transport_events<DEFER ? EV_ELECTRON_DEFER : EV_ELECTRON, R>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd,
+                                                                  nbmax, qi);
 }
 
 // The electron kernel of the engine: interactions in a kernel of their own
 // (D.defer_interact) or in place.
-static TransportKernel electron_kernel(const omc_engine *e) {
-    return e->d32.d.defer_interact ? k_electron_step<true> : k_electron_step<false>;
+template <typename R = float>
+static TransportKernelT<R> electron_kernel(const omc_engine *e) {
+    return e->d32.d.defer_interact ? k_electron_step<true, R> : k_electron_step<false, R>;
 }
 
 // Discrete interactions of the electrons the electron kernel left at their
 // interaction sites (D.defer_interact): the samplers run in a kernel of
 // their own, so the transport kernel's code stays small.
-__global__ void __launch_bounds__(EV_MAX_BLOCK) k_electron_interact(DevData<float> D, Queue in, Queue outP,
-                                                           Queue outE, double *tallies, long nvox, Ctl *ctl,
-                                                           uint32_t seedw, int *live, int nbmax, Queue qi) {
-    transport_events<EV_INTERACT>(D, in, outP, outE, tallies, nvox, ctl, seedw, live, nbmax, qi);
+template <typename R = float>
+__global__ void __launch_bounds__(EV_MAX_BLOCK) k_electron_interact(DevData<R> D, QueueT<R> in, QueueT<R> outP,
+                                                           QueueT<R> outE, double *tallies, long nvox, Ctl *ctl,
+                                                           uint32_t seedw, ServeDev *sd, int nbmax, QueueT<R> qi) {
+    transport_events<EV_INTERACT, R>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd, nbmax, qi);
 }
 
 // ------------------------------------------------------------ drain
@@ -460,32 +527,33 @@ constexpr int DRAIN_STACK = 48;
 // particles (1.2 % faster on slab64 than 8 blocks at 64 registers).
 constexpr int DRAIN_BLOCK = 128;
 
+template <typename R>
 struct DrainPart {
-    Part<float> p;
+    Part<R> p;
     uint32_t k0, k1, pos;
     int sp;       // splitting state (-1: not yet split)
     float sr;
 };
 
 // STATS (profiled runs): record the largest sub-history a thread ran.
-template <bool SPLIT, bool STATS = false>
-__global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<float> D, Queue qP, Queue qE, double *tallies,
+template <bool SPLIT, bool STATS = false, typename R = float>
+__global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<R> D, QueueT<R> qP, QueueT<R> qE, double *tallies,
                                                         long nvox, Ctl *ctl, uint32_t seedw) {
     constexpr int MAXOUT = SPLIT ? EV_MAXOUT_SPLIT : EV_MAXOUT;
     const int np = queue_size(qP), ne = queue_size(qE);
     const int n = np + ne;
-    DrainPart st[DRAIN_STACK];
+    DrainPart<R> st[DRAIN_STACK];
     unsigned flags = 0;
     unsigned long long c_ev[2] = {0, 0}, c_steps[2] = {0, 0}, c_cross[2] = {0, 0}, c_dep[2] = {0, 0},
                        c_atom[2] = {0, 0};
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const Queue &q = t < np ? qP : qE;
+        const QueueT<R> &q = t < np ? qP : qE;
         int tag = 0;
         const int qi = queue_index(q, t < np ? t : t - np);
         qload(q, qi, st[0].p, tag, st[0].k0, st[0].k1, st[0].pos);
         st[0].sp = (SPLIT && q.sp) ? q.sp[qi] : -1;
         st[0].sr = (SPLIT && q.sr) ? q.sr[qi] : 0.f;
-        EvEnv<MAXOUT> g;
+        EvEnv<MAXOUT, R> g;
         g.tally = tallies + (long)(tag >> 2) * nvox;
         g.pend_ir = -1;
         g.pend_e = 0.0;
@@ -503,8 +571,8 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<float> D, Queu
                 g.flags |= ERR_LOOP;
                 break;
             }
-            DrainPart &e = st[top];
-            Part<float> p = e.p;
+            DrainPart<R> &e = st[top];
+            Part<R> p = e.p;
             const uint64_t pkey = ((uint64_t)e.k1 << 32) | e.k0;
             g.rng.init(pkey, seedw, e.pos);
             g.nout = 0;
@@ -515,8 +583,8 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<float> D, Queu
             int sp = e.sp;
             float sr = e.sr;
             bool alive;
-            if (kind == 1) alive = electron_step<float, EvEnv<MAXOUT>, false>(D, g, p) == E_ALIVE;
-            else if (SPLIT) alive = split_event(D, g, p, sp, sr);
+            if (kind == 1) alive = electron_step<R, EvEnv<MAXOUT, R>, false>(D, g, p) == E_ALIVE;
+            else if constexpr (SPLIT) alive = split_event(D, g, p, sp, sr);
             else alive = D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p);
             c_ev[kind]++;
             x_steps += g.work;
@@ -527,7 +595,7 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<float> D, Queu
                 g.flags |= ERR_NAN;
                 alive = false;
             }
-            if (alive && p.iq == 0 && p.wt == 0.f) alive = false;
+            if (alive && p.iq == 0 && p.wt == R(0)) alive = false;
             if (alive) {
                 e.p = p;
                 e.pos = g.rng.position();
@@ -538,12 +606,12 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<float> D, Queu
                 first_alive = first_alive && !first;
             }
             for (int k = 0; k < g.nout; k++) {
-                const Part<float> &s2 = g.out[k];
+                const Part<R> &s2 = g.out[k];
                 if (!(s2.e == s2.e && s2.x == s2.x && s2.u == s2.u)) {
                     g.flags |= ERR_NAN;
                     continue;
                 }
-                if (s2.iq == 0 && s2.wt == 0.f) continue;
+                if (s2.iq == 0 && s2.wt == R(0)) continue;
                 if (top + 1 >= DRAIN_STACK) {
                     g.flags |= ERR_STACK;
                     continue;
@@ -578,7 +646,8 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<float> D, Queu
     }
 }
 
-__global__ void k_source(DevData<float> D, BeamSrc<float> S, Queue qP, Queue qE, Ctl *ctl, long long nper,
+template <typename R = float>
+__global__ void k_source(DevData<R> D, BeamSrc<R> S, QueueT<R> qP, QueueT<R> qE, Ctl *ctl, long long nper,
                          uint64_t seed, uint32_t seedw) {
     int n = ctl->inject;
     long long base = ctl->hist_base;
@@ -587,15 +656,15 @@ __global__ void k_source(DevData<float> D, BeamSrc<float> S, Queue qP, Queue qE,
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         unsigned active = __activemask();
         long long h = base + i;
-        SrcEnv g;
+        SrcEnv<R> g;
         uint64_t key = mix64(seed ^ (uint64_t)h * 0x9E3779B97F4A7C15ull);
         g.rng.init(key, seedw);
-        float ein;
-        Part<float> p = beam_primary(D, S, g, ein);
+        R ein;
+        Part<R> p = beam_primary(D, S, g, ein);
         es += ein;
         int slot = (int)(h / nper);
         int ip = warp_append(qP, p.iq == 0, false, active, flags);
-        int ie = warp_append(qE, p.iq != 0, ctl->esplit > 0.f && p.e > ctl->esplit, active, flags);
+        int ie = warp_append(qE, p.iq != 0, ctl->esplit > 0.f && p.e > (R)ctl->esplit, active, flags);
         if (ip >= 0) qstore(qP, ip, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.position());
         if (ie >= 0) qstore(qE, ie, p, slot, (uint32_t)key, (uint32_t)(key >> 32), g.rng.position());
     }
@@ -659,18 +728,54 @@ __global__ void k_plan(Ctl *ctl, int iph, int iel, PlanCfg c) {
 }
 
 // ------------------------------------------------------------------ host
-static int alloc_queue(omc_engine *e, DBuf &b, Queue &q, int cap, int *count, int *count_hi) {
-    size_t per = (size_t)cap * 4;
-    int rc = b.alloc(per * 13);
+// The event state of precision R: the FP32 form's or the FP64 form's.
+template <typename R>
+EventStateT<R> *&state_of(omc_engine *e);
+template <>
+EventStateT<float> *&state_of<float>(omc_engine *e) {
+    return e->ev;
+}
+template <>
+EventStateT<double> *&state_of<double>(omc_engine *e) {
+    return e->ev64;
+}
+template <typename R>
+const EventStateT<R> &state(const omc_engine *e) {
+    return *state_of<R>(const_cast<omc_engine *>(e));
+}
+
+// Tables and flags the event kernels of precision R run with.  The FP64
+// event form uses the FP64 tables with the event form's options (re-drawn
+// interaction distance, deferred interactions, delta tracking) instead of
+// the plain form's.
+template <typename R>
+DevData<R> event_data(const omc_engine *e);
+template <>
+DevData<float> event_data<float>(const omc_engine *e) {
+    return e->d32.d;
+}
+template <>
+DevData<double> event_data<double>(const omc_engine *e) {
+    DevData<double> d = e->d64.d;
+    d.chsteps = e->d32.d.chsteps;
+    d.defer_interact = e->d32.d.defer_interact;
+    d.woodcock = d.uniform && e->d32.d.woodcock ? 1 : 0;
+    d.nsplit = 1;
+    return d;
+}
+
+template <typename R>
+static int alloc_queue(omc_engine *e, DBuf &b, QueueT<R> &q, int cap, int *count, int *count_hi) {
+    // pos and dir: 4 values of R each; id: 16 bytes; ctr: 4 bytes (every
+    // array starts on a 16-byte boundary for any cap)
+    const size_t v4 = (size_t)cap * 4 * sizeof(R), per = (size_t)cap * 4;
+    int rc = b.alloc(2 * v4 + 5 * per);
     if (rc) return set_err(e, rc, "event queue allocation failed");
     char *p = (char *)b.p;
-    float **f[8] = {&q.x, &q.y, &q.z, &q.u, &q.v, &q.w, &q.e, &q.wt};
-    for (int i = 0; i < 8; i++) *f[i] = (float *)(p + per * i);
-    q.ir = (int *)(p + per * 8);
-    q.tag = (int *)(p + per * 9);
-    q.k0 = (uint32_t *)(p + per * 10);
-    q.k1 = (uint32_t *)(p + per * 11);
-    q.ctr = (uint32_t *)(p + per * 12);
+    q.pos = (typename QVec<R>::T *)p;
+    q.dir = (typename QVec<R>::T *)(p + v4);
+    q.id = (uint4 *)(p + 2 * v4);
+    q.ctr = (uint32_t *)(p + 2 * v4 + 4 * per);
     q.count = count;
     q.count_hi = count_hi;
     q.cap = cap;
@@ -679,37 +784,50 @@ static int alloc_queue(omc_engine *e, DBuf &b, Queue &q, int cap, int *count, in
     return OMC_OK;
 }
 
-// The photon kernel of the engine: split photons when nsplit > 1.
-static TransportKernel photon_kernel(const omc_engine *e) {
-    return e->d32.d.nsplit > 1 ? k_photon_split_step : k_photon_step;
+// The photon kernel of the engine: split photons when nsplit > 1 (FP32
+// form only).
+template <typename R = float>
+static TransportKernelT<R> photon_kernel(const omc_engine *e);
+template <>
+TransportKernelT<float> photon_kernel<float>(const omc_engine *e) {
+    return e->d32.d.nsplit > 1 ? k_photon_split_step : k_photon_step<float>;
+}
+template <>
+TransportKernelT<double> photon_kernel<double>(const omc_engine *) {
+    return k_photon_step<double>;
 }
 
 // Resident blocks per SM of the transport kernels -> one-wave grids.
-static void size_grids(omc_engine *e, EventState &S) {
+template <typename R>
+static void size_grids(omc_engine *e, EventStateT<R> &S) {
     int bp = 0, be = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, photon_kernel(e), S.block, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, electron_kernel(e), S.block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, photon_kernel<R>(e), S.block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, electron_kernel<R>(e), S.block, 0);
     S.grid_p = e->sm_count * std::max(1, bp);
     S.grid_e = e->sm_count * std::max(1, be);
     int bi = 0, bd = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_electron_interact, S.block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_electron_interact<R>, S.block, 0);
     S.grid_i = e->sm_count * std::max(1, bi);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_drain<false>, DRAIN_BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_drain<false, false, R>, DRAIN_BLOCK, 0);
     S.drain_lanes = e->sm_count * std::max(1, bd) * DRAIN_BLOCK;
     S.lanes = S.grid_e * S.block;
 }
 
 // The interaction queue, allocated when the engine first needs it.
-int event_interact_queue(omc_engine *e) {
-    EventState &S = *e->ev;
+template <typename R>
+static int event_interact_queue_t(omc_engine *e) {
+    EventStateT<R> &S = *state_of<R>(e);
     if (!e->d32.d.defer_interact || S.int_buf.p) return OMC_OK;
     return alloc_queue(e, S.int_buf, S.qi, S.cap, &S.ctl_d->cnt_int, &S.ctl_d->cnt_int_hi);
 }
+int event_interact_queue(omc_engine *e) { return event_interact_queue_t<float>(e); }
 
-int event_prepare(omc_engine *e) {
-    if (e->ev && e->ev->ready) return OMC_OK;
-    if (!e->ev) e->ev = new EventState();
-    EventState &S = *e->ev;
+template <typename R>
+static int event_prepare_t(omc_engine *e) {
+    EventStateT<R> *&sp = state_of<R>(e);
+    if (sp && sp->ready) return OMC_OK;
+    if (!sp) sp = new EventStateT<R>();
+    EventStateT<R> &S = *sp;
     long cap = e->opt.queue_capacity > 0 ? e->opt.queue_capacity : (1L << 22);
     S.cap = (int)std::min(cap, (long)(1L << 30));
     // warps fetch work 32 particles at a time: whole warps per block, at
@@ -725,16 +843,16 @@ int event_prepare(omc_engine *e) {
     S.esplit = e->opt.electron_split > 0 ? e->opt.electron_split + D_RM : 0.0;
     int rc = S.ctl.alloc(sizeof(Ctl));
     if (rc) return set_err(e, rc, "control block allocation failed");
-    S.ctl_d = S.ctl.as<Ctl>();
+    S.ctl_d = S.ctl.template as<Ctl>();
     for (int i = 0; i < 4; i++)
         if ((rc = alloc_queue(e, S.buf[i], S.q[i], S.cap, &S.ctl_d->cnt[i], &S.ctl_d->cnt_hi[i]))) return rc;
-    if (e->d32.d.nsplit > 1) {
+    if (e->d32.d.nsplit > 1 && sizeof(R) == 4) {
         // splitting state of the two photon queues (A and B)
         for (int k = 0; k < 2; k++) {
             size_t per = (size_t)S.cap * 4;
             if ((rc = S.split_buf[k].alloc(per * 2))) return set_err(e, rc, "splitting state allocation failed");
-            Queue &q = S.q[2 * k];
-            q.sp = S.split_buf[k].as<int>();
+            QueueT<R> &q = S.q[2 * k];
+            q.sp = S.split_buf[k].template as<int>();
             q.sr = (float *)((char *)S.split_buf[k].p + per);
         }
     }
@@ -745,6 +863,7 @@ int event_prepare(omc_engine *e) {
     S.ready = true;
     return OMC_OK;
 }
+int event_prepare(omc_engine *e) { return event_prepare_t<float>(e); }
 
 // The transport kernels of one cycle after its source kernel.  Profiled
 // (`ev`): one after the other on the engine's stream, an event after each.
@@ -755,20 +874,22 @@ int event_prepare(omc_engine *e) {
 // the SMs that the electron kernel's last blocks leave (4-5 % faster on
 // slab64; same dose).  The side stream joins the engine's stream before the
 // next cycle.
+template <typename R = float>
 static void launch_transport(omc_engine *e, int iph, int iel, int oph, int oel, double *tallies, uint32_t seedw,
-                             int *live, int nbmax, cudaEvent_t *ev) {
-    EventState &S = *e->ev;
+                             ServeDev *sd, int nbmax, cudaEvent_t *ev) {
+    EventStateT<R> &S = *state_of<R>(e);
     const long nvox = e->ph.nvox();
+    const DevData<R> D = event_data<R>(e);
     auto photons = [&](cudaStream_t st) {
-        photon_kernel(e)<<<S.grid_p, S.block, 0, st>>>(e->d32.d, S.q[iph], S.q[oph], S.q[oel], tallies, nvox,
-                                                       S.ctl_d, seedw, live, nbmax, S.qi);
+        photon_kernel<R>(e)<<<S.grid_p, S.block, 0, st>>>(D, S.q[iph], S.q[oph], S.q[oel], tallies, nvox, S.ctl_d,
+                                                          seedw, sd, nbmax, S.qi);
     };
     auto electrons = [&]() {
-        electron_kernel(e)<<<S.grid_e, S.block, 0, e->stream>>>(e->d32.d, S.q[iel], S.q[oph], S.q[oel], tallies,
-                                                                 nvox, S.ctl_d, seedw, live, nbmax, S.qi);
-        if (e->d32.d.defer_interact)
-            k_electron_interact<<<S.grid_i, S.block, 0, e->stream>>>(e->d32.d, S.qi, S.q[oph], S.q[oel], tallies,
-                                                                     nvox, S.ctl_d, seedw, live, nbmax, S.qi);
+        electron_kernel<R>(e)<<<S.grid_e, S.block, 0, e->stream>>>(D, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
+                                                                    S.ctl_d, seedw, sd, nbmax, S.qi);
+        if (D.defer_interact)
+            k_electron_interact<R><<<S.grid_i, S.block, 0, e->stream>>>(D, S.qi, S.q[oph], S.q[oel], tallies, nvox,
+                                                                        S.ctl_d, seedw, sd, nbmax, S.qi);
     };
     if (ev || !S.side) {
         photons(e->stream);
@@ -796,8 +917,7 @@ int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, i
             return set_err(e, OMC_E_ARG, "block must be a multiple of 32, at most 256");
         e->opt.block = block;
     }
-    if (e->ev && e->ev->ready) {
-        EventState &S = *e->ev;
+    auto apply = [&](auto &S) {
         S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 1;
         S.boost = e->opt.tail_boost > 0 ? e->opt.tail_boost : 32;
         S.inflight = e->opt.inflight > 0 ? e->opt.inflight : (1LL << 20);
@@ -805,12 +925,15 @@ int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, i
         S.block = e->opt.block > 0 ? std::min(EV_MAX_BLOCK, e->opt.block) : 256;
         S.grid = e->sm_count * std::max(1, 2048 / S.block);
         size_grids(e, S);
-    }
+    };
+    if (e->ev && e->ev->ready) apply(*e->ev);
+    if (e->ev64 && e->ev64->ready) apply(*e->ev64);
     return OMC_OK;
 }
 
-PlanCfg plan_cfg(const omc_engine *e, long long target) {
-    const EventState &S = *e->ev;
+template <typename R>
+static PlanCfg plan_cfg_t(const omc_engine *e, long long target) {
+    const EventStateT<R> &S = state<R>(e);
     PlanCfg c;
     c.target = target;
     c.cap = S.cap;
@@ -818,30 +941,35 @@ PlanCfg plan_cfg(const omc_engine *e, long long target) {
     c.boost = S.boost;
     c.tsteps = S.tsteps;
     c.esplit = (float)S.esplit;
-    c.pweight = std::max(1, e->d32.d.nsplit);
+    c.pweight = sizeof(R) == 4 ? std::max(1, e->d32.d.nsplit) : 1;
     return c;
 }
+PlanCfg plan_cfg(const omc_engine *e, long long target) { return plan_cfg_t<float>(e, target); }
 
 void event_release(omc_engine *e) {
     delete e->ev;
     e->ev = nullptr;
+    delete e->ev64;
+    e->ev64 = nullptr;
 }
 
 // One transport cycle with input buffers `in` (0 = A, 1 = B).  With `ev`
 // (profiling) the launches are sequential and an event is recorded before
 // each and after the last.
-static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, double *tallies, long nper, uint64_t seed,
+template <typename R = float>
+static void launch_cycle(omc_engine *e, int in, const BeamSrc<R> &src, double *tallies, long nper, uint64_t seed,
                          long long target, cudaEvent_t *ev = nullptr) {
-    EventState &S = *e->ev;
+    EventStateT<R> &S = *state_of<R>(e);
     int iph = in == 0 ? 0 : 2, iel = iph + 1;
     int oph = in == 0 ? 2 : 0, oel = oph + 1;
     uint32_t seedw = (uint32_t)(seed >> 32);
     if (ev) cudaEventRecord(ev[0], e->stream);
-    k_plan<<<1, 1, 0, e->stream>>>(S.ctl_d, iph, iel, plan_cfg(e, target));
+    k_plan<<<1, 1, 0, e->stream>>>(S.ctl_d, iph, iel, plan_cfg_t<R>(e, target));
     if (ev) cudaEventRecord(ev[1], e->stream);
-    k_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, src, S.q[iph], S.q[iel], S.ctl_d, nper, seed, seedw);
+    k_source<R><<<S.grid, S.block, 0, e->stream>>>(event_data<R>(e), src, S.q[iph], S.q[iel], S.ctl_d, nper, seed,
+                                                   seedw);
     if (ev) cudaEventRecord(ev[2], e->stream);
-    launch_transport(e, iph, iel, oph, oel, tallies, seedw, nullptr, 1, ev);
+    launch_transport<R>(e, iph, iel, oph, oel, tallies, seedw, nullptr, 1, ev);
     if (ev) cudaEventRecord(ev[4], e->stream);
 }
 
@@ -851,24 +979,31 @@ static void launch_cycle(omc_engine *e, int in, const BeamSrc<float> &src, doubl
 // whole remaining cascade in one thread, so it pays only once the cycles
 // are mostly idle (measured on slab64: ≈40 k best of 5 k - 1 M particles,
 // for 10^6- and 10^7-history runs alike).
-long long drain_threshold(const omc_engine *e) {
-    const EventState &S = *e->ev;
+template <typename R>
+static long long drain_threshold_t(const omc_engine *e) {
+    const EventStateT<R> &S = state<R>(e);
     if (e->opt.drain_particles < 0) return 0;
     return e->opt.drain_particles > 0 ? e->opt.drain_particles : S.drain_lanes / 2;
 }
+long long drain_threshold(const omc_engine *e) { return drain_threshold_t<float>(e); }
 
 // The drain over the queues `iph`/`iph + 1` holding `left` particles, on
 // the streams of the cycles that filled them (seed word `seedw`); `stats`
 // records its largest sub-history.
+template <typename R = float>
 static void launch_drain(omc_engine *e, int iph, long long left, double *tallies, uint32_t seedw,
                          bool stats = false) {
-    EventState &S = *e->ev;
+    EventStateT<R> &S = *state_of<R>(e);
     long long g = (left + DRAIN_BLOCK - 1) / DRAIN_BLOCK;
     g = std::max(1LL, std::min(g, (long long)S.drain_lanes / DRAIN_BLOCK * 4));
-    auto kd = e->d32.d.nsplit > 1 ? (stats ? k_drain<true, true> : k_drain<true, false>)
-                                  : (stats ? k_drain<false, true> : k_drain<false, false>);
-    kd<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(e->d32.d, S.q[iph], S.q[iph + 1], tallies, e->ph.nvox(), S.ctl_d,
-                                              seedw);
+    const DevData<R> D = event_data<R>(e);
+    void (*kd)(DevData<R>, QueueT<R>, QueueT<R>, double *, long, Ctl *, uint32_t);
+    if constexpr (sizeof(R) == 4)
+        kd = D.nsplit > 1 ? (stats ? k_drain<true, true, R> : k_drain<true, false, R>)
+                          : (stats ? k_drain<false, true, R> : k_drain<false, false, R>);
+    else
+        kd = stats ? k_drain<false, true, R> : k_drain<false, false, R>;
+    kd<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(D, S.q[iph], S.q[iph + 1], tallies, e->ph.nvox(), S.ctl_d, seedw);
 }
 
 // Profiled transport: cycles launched one by one with events around each
@@ -935,39 +1070,42 @@ static int run_profiled(omc_engine *e, const BeamSrc<float> &src, double *tallie
     return rc;
 }
 
+template <typename R>
 int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint64_t seed, double *sum, double *sum2,
                    double *src_energy, KernelStats &ks) {
-    int rc = event_prepare(e);
-    if (!rc) rc = event_interact_queue(e);
+    if (sizeof(R) == 8 && e->d32.d.nsplit > 1)
+        return set_err(e, OMC_E_RANGE, "the FP64 event form has no photon splitting (nsplit > 1)");
+    int rc = event_prepare_t<R>(e);
+    if (!rc) rc = event_interact_queue_t<R>(e);
     if (rc) return rc;
-    EventState &S = *e->ev;
+    EventStateT<R> &S = *state_of<R>(e);
     long nvox = e->ph.nvox();
     DBuf &tal = e->run_tal, &cdf = e->run_cdf32;
     if ((rc = tal.reserve((size_t)nbatch * nvox * 8))) return set_err(e, rc, "batch tallies allocation failed");
     cudaMemsetAsync(tal.p, 0, (size_t)nbatch * nvox * 8, e->stream);
     int ncdf = b->energy.n;
-    BeamSrc<float> src = beam_setup<float>(e, b);
+    BeamSrc<R> src = beam_setup<R>(e, b);
     if (ncdf > 0) {
-        std::vector<float> c(b->energy.cdf1, b->energy.cdf1 + ncdf);
+        std::vector<R> c(b->energy.cdf1, b->energy.cdf1 + ncdf);
         c.insert(c.end(), b->energy.cdf2, b->energy.cdf2 + ncdf);
-        if ((rc = cdf.reserve(c.size() * 4))) return set_err(e, rc, "alloc");
-        cudaMemcpyAsync(cdf.p, c.data(), c.size() * 4, cudaMemcpyHostToDevice, e->stream);
-        src.cdf1 = cdf.as<float>();
-        src.cdf2 = cdf.as<float>() + ncdf;
+        if ((rc = cdf.reserve(c.size() * sizeof(R)))) return set_err(e, rc, "alloc");
+        cudaMemcpyAsync(cdf.p, c.data(), c.size() * sizeof(R), cudaMemcpyHostToDevice, e->stream);
+        src.cdf1 = cdf.as<R>();
+        src.cdf2 = cdf.as<R>() + ncdf;
     }
     Ctl c0{};
     c0.hist_total = (long long)nper * nbatch;
     cudaMemcpyAsync(S.ctl_d, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, e->stream);
     long long target = std::min<long long>((long long)S.cap / 2, S.inflight);
 
-    if (e->opt.profile) {
+    if (e->opt.profile && sizeof(R) == 4) {
         Ctl h{};
         long cycles = 0;
         cudaEvent_t t0, t1;
         cudaEventCreate(&t0);
         cudaEventCreate(&t1);
         cudaEventRecord(t0, e->stream);
-        rc = run_profiled(e, src, tal.as<double>(), nper, seed, target, h, cycles);
+        if constexpr (sizeof(R) == 4) rc = run_profiled(e, src, tal.as<double>(), nper, seed, target, h, cycles);
         for (int ib = 0; ib < nbatch && rc == OMC_OK; ib++)
             rc = fold(e, tal.as<double>() + (size_t)ib * nvox, sum, sum2, nvox, 1.0);
         cudaEventRecord(t1, e->stream);
@@ -997,8 +1135,8 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     if ((rc = cuda_check(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal), "capture"))) return rc;
-    launch_cycle(e, 0, src, tal.as<double>(), nper, seed, target);
-    launch_cycle(e, 1, src, tal.as<double>(), nper, seed, target);
+    launch_cycle<R>(e, 0, src, tal.as<double>(), nper, seed, target);
+    launch_cycle<R>(e, 1, src, tal.as<double>(), nper, seed, target);
     if ((rc = cuda_check(e, cudaStreamEndCapture(e->stream, &graph), "end capture"))) return rc;
     if ((rc = cuda_check(e, cudaGraphInstantiate(&exec, graph, 0), "graph instantiate"))) {
         cudaGraphDestroy(graph);
@@ -1011,7 +1149,7 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
     Ctl h{};
     long graphs = 0;
     int per_check = 4;
-    const long long dthr = drain_threshold(e);
+    const long long dthr = drain_threshold_t<R>(e);
     int drains = 0;
     for (;;) {
         for (int k = 0; k < per_check; k++) cudaGraphLaunch(exec, e->stream);
@@ -1029,7 +1167,7 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
             long long left = (long long)std::min(h.cnt[0] + h.cnt_hi[0], S.cap) +
                              std::min(h.cnt[1] + h.cnt_hi[1], S.cap);
             if (left <= dthr) {
-                launch_drain(e, 0, left, tal.as<double>(), (uint32_t)(seed >> 32));
+                launch_drain<R>(e, 0, left, tal.as<double>(), (uint32_t)(seed >> 32));
                 drains = 1;
                 if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "drain"))) break;
                 cudaMemcpy(&h, S.ctl_d, sizeof(Ctl), cudaMemcpyDeviceToHost);
@@ -1065,37 +1203,96 @@ int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint
     cudaMemcpyAsync(src_energy, &S.ctl_d->src_energy, 8, cudaMemcpyDeviceToDevice, e->stream);
     return OMC_OK;
 }
+template int event_run_beam<float>(omc_engine *, const omc_beam *, long, int, uint64_t, double *, double *, double *,
+                                   KernelStats &);
+template int event_run_beam<double>(omc_engine *, const omc_beam *, long, int, uint64_t, double *, double *, double *,
+                                    KernelStats &);
 
 // ============================================================== serving
-// Histories to inject this cycle across the admitted requests, first come
-// first served, keeping `target` particles in flight.
-__global__ void k_serve_plan(ServeDev *sd, Ctl *ctl, int iph, int iel, PlanCfg c) {
-    const int cap = c.cap;
-    long long np, ne;
-    plan_queues(ctl, iph, iel, cap, np, ne);
-    long long room = (c.target - (np * c.pweight + ne)) / c.pweight;
-    long long qroom = (long long)cap - (np > ne ? np : ne);
-    if (room > qroom) room = qroom;
-    int nplan = 0;
-    long long cum = 0;
-    for (int k = 0; k < sd->norder && room - cum > 0; k++) {
-        int s = sd->order[k];
-        ServeReq &r = sd->req[s];
-        if (r.kind < 0) continue;
-        long long rem = r.nhist - r.next;
-        if (rem <= 0) continue;
-        long long take = rem < room - cum ? rem : room - cum;
-        sd->plan_slot[nplan] = s;
-        sd->plan_first[nplan] = r.next;
-        sd->plan_cum[nplan] = (int)cum;
-        cum += take;
-        r.next += take;
-        nplan++;
+// Inclusive prefix sum over the block (blockDim.x a multiple of 32, at most
+// 1024) of one value per thread.
+template <typename T>
+__device__ __forceinline__ T block_inclusive_scan(T v, T *warp_tot) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+        T t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
     }
-    sd->plan_cum[nplan] = (int)cum;
-    sd->nplan = nplan;
-    sd->inject_total = (int)cum;
-    plan_budget(ctl, ne, c);
+    if (lane == 31) warp_tot[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        T w = lane < nw ? warp_tot[lane] : T(0);
+        for (int o = 1; o < 32; o <<= 1) {
+            T t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < nw) warp_tot[lane] = w;
+    }
+    __syncthreads();
+    if (wid > 0) v += warp_tot[wid - 1];
+    __syncthreads();
+    return v;
+}
+
+// Histories to inject this cycle across the admitted requests, first come
+// first served, keeping `target` particles in flight.  One block of
+// SERVE_MAX threads, one per position in the admission order: request k
+// takes min(its remaining histories, room left after requests 0..k-1),
+// found by a prefix sum of the remaining histories.
+__global__ void __launch_bounds__(SERVE_MAX) k_serve_plan(ServeDev *sd, Ctl *ctl, int iph, int iel, PlanCfg c) {
+    __shared__ long long s_room;
+    __shared__ long long warp_ll[SERVE_MAX / 32];
+    __shared__ int warp_i[SERVE_MAX / 32];
+    const int cap = c.cap;
+    if (threadIdx.x == 0) {
+        long long np, ne;
+        plan_queues(ctl, iph, iel, cap, np, ne);
+        long long room = (c.target - (np * c.pweight + ne)) / c.pweight;
+        long long qroom = (long long)cap - (np > ne ? np : ne);
+        if (room > qroom) room = qroom;
+        s_room = room;
+        plan_budget(ctl, ne, c);
+    }
+    __syncthreads();
+    const long long room = s_room;
+    const int k = threadIdx.x;
+    int slot = -1;
+    long long rem = 0, next = 0;
+    if (k < sd->norder) {
+        slot = sd->order[k];
+        const ServeReq &r = sd->req[slot];
+        if (r.kind >= 0 && r.nhist > r.next) {
+            rem = r.nhist - r.next;
+            next = r.next;
+        }
+    }
+    const long long before = block_inclusive_scan(rem, warp_ll) - rem;
+    long long take = room - before;
+    take = take < 0 ? 0 : (take > rem ? rem : take);
+    const int planned = take > 0;
+    const int pos = block_inclusive_scan(planned, warp_i) - planned;
+    if (planned) {
+        // every request before this one got all it asked for: `before` is
+        // the injections planned ahead of it
+        sd->plan_slot[pos] = slot;
+        sd->plan_first[pos] = next;
+        sd->plan_cum[pos] = (int)before;
+        sd->req[slot].next = next + take;
+    }
+    if (slot >= 0) {
+        // the tail of a request whose histories are all in: a larger budget
+        const bool tail = rem == take && sd->tail_particles > 0 && sd->live[slot] <= sd->tail_particles;
+        sd->boost[slot] = tail ? sd->tail_boost : 1;
+    }
+    // the last thread sees the totals
+    if (k == blockDim.x - 1) {
+        const long long total_rem = before + rem;
+        const long long total = total_rem < room ? total_rem : (room > 0 ? room : 0);
+        const int nplan = pos + planned;
+        sd->plan_cum[nplan] = (int)total;
+        sd->nplan = nplan;
+        sd->inject_total = (int)total;
+    }
 }
 
 // Primaries of the planned histories; each history's stream key is derived
@@ -1116,7 +1313,7 @@ __global__ void k_serve_source(DevData<float> D, ServeDev *sd, Queue qP, Queue q
         const ServeReq &r = sd->req[s];
         long long local = sd->plan_first[lo] + (i - sd->plan_cum[lo]);
         uint64_t key = mix64(r.seed ^ (uint64_t)local * 0x9E3779B97F4A7C15ull);
-        SrcEnv g;
+        SrcEnv<float> g;
         g.rng.init(key, seedw);
         float ein;
         Part<float> p = r.kind == 0 ? beam_primary(D, sd->beam[s], g, ein) : beamlet_primary(D, sd->bl[s], r.bixel, g, ein);
@@ -1136,9 +1333,9 @@ void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, in
     int iph = in == 0 ? 0 : 2, iel = iph + 1;
     int oph = in == 0 ? 2 : 0, oel = oph + 1;
     const uint32_t seedw = SERVE_SEEDW;
-    k_serve_plan<<<1, 1, 0, e->stream>>>(sd, S.ctl_d, iph, iel, plan_cfg(e, target));
+    k_serve_plan<<<1, SERVE_MAX, 0, e->stream>>>(sd, S.ctl_d, iph, iel, plan_cfg(e, target));
     k_serve_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, sd, S.q[iph], S.q[iel], S.ctl_d, nbmax, seedw);
-    launch_transport(e, iph, iel, oph, oel, tallies, seedw, sd->live, nbmax, nullptr);
+    launch_transport(e, iph, iel, oph, oel, tallies, seedw, sd, nbmax, nullptr);
 }
 
 // A serving cycle launched on its own with an event around each kernel
@@ -1153,11 +1350,11 @@ int serve_profiled_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, i
     cudaEvent_t ev[5];
     for (auto &x : ev) cudaEventCreate(&x);
     cudaEventRecord(ev[0], e->stream);
-    k_serve_plan<<<1, 1, 0, e->stream>>>(sd, S.ctl_d, iph, iel, plan_cfg(e, target));
+    k_serve_plan<<<1, SERVE_MAX, 0, e->stream>>>(sd, S.ctl_d, iph, iel, plan_cfg(e, target));
     cudaEventRecord(ev[1], e->stream);
     k_serve_source<<<S.grid, S.block, 0, e->stream>>>(e->d32.d, sd, S.q[iph], S.q[iel], S.ctl_d, nbmax, seedw);
     cudaEventRecord(ev[2], e->stream);
-    launch_transport(e, iph, iel, oph, oel, tallies, seedw, sd->live, nbmax, ev);
+    launch_transport(e, iph, iel, oph, oel, tallies, seedw, sd, nbmax, ev);
     cudaEventRecord(ev[4], e->stream);
     int rc = cuda_check(e, cudaEventSynchronize(ev[4]), "profiled serving cycle");
     if (!rc) {

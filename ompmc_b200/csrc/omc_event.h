@@ -5,17 +5,32 @@
 
 namespace omc {
 
-// Structure-of-arrays particle queue in device memory.  `tag` packs the
-// charge (iq+1, 2 bits) and the tally slot (upper bits); k0/k1 are the
-// particle's Philox stream key and ctr its stream position (numbers drawn).
-// Entries fill from both ends: `count` entries from index 0 up and
-// `count_hi` entries from index cap-1 down (electron queues put particles
-// above the regroup energy at the top, so that warps see particles of one
-// kind).
-struct Queue {
-    float *x, *y, *z, *u, *v, *w, *e, *wt;
-    int *ir, *tag;
-    uint32_t *k0, *k1, *ctr;
+// Particle queue in device memory: four arrays of 16-, 16-, 16- and 4-byte
+// elements (FP32 form), so a warp moves a particle's 52 bytes with three
+// 128-bit and one 32-bit coalesced access each way: pos = (x, y, z, u),
+// dir = (v, w, e, wt), id = (ir, tag, k0, k1), ctr.  The FP64 event form
+// keeps pos and dir in double (84 bytes per particle).  `tag` packs the charge (iq+1, 2 bits)
+// and the tally slot (upper bits); k0/k1 are the particle's Philox stream
+// key and ctr its stream position (numbers drawn).  Entries fill from both
+// ends: `count` entries from index 0 up and `count_hi` entries from index
+// cap-1 down (electron queues put particles above the regroup energy at
+// the top, so that warps see particles of one kind).
+template <typename R>
+struct QVec;
+template <>
+struct QVec<float> {
+    using T = float4;
+};
+template <>
+struct QVec<double> {
+    using T = double4;   // two 128-bit accesses
+};
+
+template <typename R>
+struct QueueT {
+    typename QVec<R>::T *pos, *dir;
+    uint4 *id;
+    uint32_t *ctr;
     // photon splitting state (photon queues of engines with nsplit > 1,
     // else null): -1 for a photon not yet split, else (next sub-photon << 16)
     // | surviving sub-photon; and the ray's stratification offset
@@ -25,6 +40,7 @@ struct Queue {
     int *count_hi;   // device counter of entries from the top
     int cap;
 };
+using Queue = QueueT<float>;
 
 // Cycle control block in device memory.
 struct Ctl {
@@ -67,14 +83,15 @@ struct PlanCfg {
                               // nsplit charged particles), 1 without splitting
 };
 
-struct EventState {
+template <typename R>
+struct EventStateT {
     bool ready = false;
     int cap = 0;              // per queue
     DBuf buf[4];              // photon A, electron A, photon B, electron B (13 arrays each)
     DBuf split_buf[2];        // splitting state of the photon queues (nsplit > 1)
     DBuf int_buf;             // electrons at their discrete interaction (defer_interact)
-    Queue qi;
-    Queue q[4];
+    QueueT<R> qi;
+    QueueT<R> q[4];
     DBuf ctl;
     Ctl *ctl_d = nullptr;
     int block = 256;
@@ -97,12 +114,13 @@ struct EventState {
     // beside the electron kernels of its cycle (fork/join events)
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
-    ~EventState() {
+    ~EventStateT() {
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
         if (side) cudaStreamDestroy(side);
     }
 };
+using EventState = EventStateT<float>;
 
 // ------------------------------------------------------------ serving
 constexpr int SERVE_MAX = 256;  // request slots resident on the device
@@ -123,11 +141,18 @@ struct ServeDev {
     BeamSrc<float> beam[SERVE_MAX];
     BeamletSrc<float> bl[SERVE_MAX];
     int live[SERVE_MAX];       // particles of the request in the queues
+    int boost[SERVE_MAX];      // electron budget multiplier of the request's particles this cycle
     int order[SERVE_MAX];      // active slots in admission order
     int norder;
     int nplan;
     int inject_total;
     int pad;
+    // a request whose histories are all injected and which has at most
+    // tail_particles particles left runs them with tail_boost times the
+    // cycle's electron budget (0: never), so its longest chains take fewer
+    // cycles; budgets do not change trajectories
+    int tail_particles;
+    int tail_boost;
     int plan_slot[SERVE_MAX];
     long long plan_first[SERVE_MAX];
     int plan_cum[SERVE_MAX + 1];
@@ -147,6 +172,9 @@ long long drain_threshold(const omc_engine *e);
 PlanCfg plan_cfg(const omc_engine *e, long long target);
 int event_set_params(omc_engine *e, int tsteps, int boost, long long inflight, int block, double split_kinetic);
 
+// The event form's dose run in precision R (float: FP32 transport; double:
+// the FP64 event form, OMC_EVENT_FP64).
+template <typename R>
 int event_run_beam(omc_engine *e, const omc_beam *b, long nper, int nbatch, uint64_t seed, double *sum, double *sum2,
                    double *src_energy, KernelStats &ks);
 void event_release(omc_engine *e);

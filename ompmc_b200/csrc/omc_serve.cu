@@ -27,6 +27,10 @@
 #include "omc_source.cuh"
 
 namespace omc {
+// Default tail of a served request: once its histories are all injected and
+// at most this many of its particles are left, its electrons run with the
+// engine's tail_boost times the cycle's budget.
+constexpr int SERVE_TAIL_PARTICLES = 4096;
 int finalize_dosxyz(omc_engine *e, const double *sum, const double *sum2, int nbatch, double nper, double *dose,
                     double *unc);
 int finalize_matrad(omc_engine *e, const double *sum, const double *sum2, int nbatch, double *dose, double *var);
@@ -111,6 +115,71 @@ __global__ void k_seg_write(const double *d, const double *v, long n, long segle
         }
         base += tile;
         __syncthreads();
+    }
+}
+
+// Fold, finalise and (beamlets) column maximum of one finished request in
+// one pass over its batch tallies: per voxel the batch values are summed in
+// batch order (the order of k_fold over the batches, so the result is the
+// same to the bit), the tallies are zeroed for the slot's next request, and
+// dose with its uncertainty (dosxyz, accumulateResults omc_dosxyz.c:719-799)
+// or variance of the mean (matRad, omc_matrad.c:920-1012) is written.
+// HBM traffic: nbatch tallies read and zeroed, two outputs written.
+__global__ void k_serve_finalize(double *__restrict__ tal, int nbatch, long nv, double scale, int kind,
+                                 const double *__restrict__ mass, const double *__restrict__ rho, double nper,
+                                 double *__restrict__ dose, double *__restrict__ second,
+                                 unsigned long long *dmaxbits) {
+    double m = 0.0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nv; i += (long)gridDim.x * blockDim.x) {
+        double sum = 0.0, sum2 = 0.0;
+        for (int b = 0; b < nbatch; b++) {
+            double x = tal[(size_t)b * nv + i] * scale;
+            sum += x;
+            sum2 += x * x;
+            tal[(size_t)b * nv + i] = 0.0;
+        }
+        double en, u;
+        if (kind == 0) {
+            en = sum / (double)nbatch;
+            double en2 = sum2 / (double)nbatch;
+            if (en != 0.0) {
+                u = en2 - en * en;
+                u /= (double)(nbatch - 1);
+                u = sqrt(u) / en;
+            } else {
+                en = 0.0;
+                u = 0.9999999;
+            }
+            en *= 1.602E-10 / (mass[i] * nper);
+            if (rho[i] < 0.044) {
+                en = 0.0;
+                u = 0.9999999;
+            }
+        } else {
+            double f = 1.602E-10 / mass[i];
+            en = sum * f;
+            double en2 = sum2 * f * f;
+            en /= (double)nbatch;
+            en2 /= (double)(nbatch - 1);
+            if (en != 0.0) {
+                u = en2 - en * en;
+                u /= nbatch;
+            } else {
+                en = 0.0;
+                u = 0.0;
+            }
+            if (rho[i] < 0.044) {
+                en = 0.0;
+                u = 0.0;
+            }
+            m = fmax(m, en);
+        }
+        dose[i] = en;
+        second[i] = u;
+    }
+    if (kind != 0) {
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(dmaxbits, (unsigned long long)__double_as_longlong(m));
     }
 }
 
@@ -215,6 +284,39 @@ struct omc_server {
     long long cycles = 0, drains = 0, launches = 0, finished = 0;
     std::vector<int> completed;  // finished since the last omc_server_completed
     cudaEvent_t t_start = nullptr, t_stop = nullptr;
+    // Pipelined completion check: every step copies the request table, the
+    // live counts and the queue counters into a pinned snapshot after its
+    // transport work and then processes the previous step's snapshot, which
+    // is ready once the previous work is, so the host never waits for the
+    // work it has just queued.  A snapshot is valid for a slot only if it was
+    // taken after the slot's request was admitted (slot_seq).
+    struct Snap {
+        ServeReq *req = nullptr;
+        int *live = nullptr;
+        unsigned *flags = nullptr;
+        int *qc = nullptr;     // Ctl::cnt, Ctl::cnt_hi
+        cudaEvent_t ev = nullptr;
+        long long seq = 0;     // 0: none pending
+    } snap[2];
+    void *snap_host = nullptr;
+    int cur = 0;
+    long long seq = 0;               // snapshots taken so far
+    long long drain_seq = -1;        // snapshots taken before the last drain
+    std::vector<long long> slot_seq; // snapshots taken before each slot's admission
+    cudaStream_t fin_stream = nullptr;  // finalisation, beside the transport
+    ~omc_server() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (t_start) cudaEventDestroy(t_start);
+        if (t_stop) cudaEventDestroy(t_stop);
+        if (fin_stream) {
+            cudaStreamSynchronize(fin_stream);
+            cudaStreamDestroy(fin_stream);
+        }
+        for (auto &sn : snap)
+            if (sn.ev) cudaEventDestroy(sn.ev);
+        if (snap_host) cudaFreeHost(snap_host);
+    }
     // state after the last step: particles in the queues, and whether every
     // running request had all its histories injected
     long long left = 0;
@@ -229,49 +331,48 @@ struct omc_server {
 
 namespace {
 
-// Fold, finalise and extract one finished request into host memory.
+// Fold, finalise and extract one finished request into host memory, on the
+// finalisation stream (the transport work queued on the engine's stream
+// goes on meanwhile; it does not touch this request's tallies, whose live
+// count is zero and whose histories are all injected).
 int finalize_request(omc_server *s, Request &r) {
     omc_engine *e = s->e;
+    cudaStream_t st = s->fin_stream;
     long nv = e->ph.nvox();
     int rc;
-    cudaMemsetAsync(s->f_sum, 0, nv * 8, e->stream);
-    cudaMemsetAsync(s->f_sum2, 0, nv * 8, e->stream);
     double scale = r.kind == 1 ? 1.0 / (double)r.nper : 1.0;
-    s->launches += r.nbatch + (r.kind == 0 ? 1 : 5);   // folds, finalise (+ column extraction)
-    for (int b = 0; b < r.nbatch; b++) {
-        double *w = s->tallies.as<double>() + ((size_t)r.slot * s->nbmax + b) * nv;
-        if ((rc = fold(e, w, s->f_sum, s->f_sum2, nv, scale))) return rc;
-    }
+    s->launches += r.kind == 0 ? 1 : 4;   // fused fold + finalise (+ column extraction)
+    double *tal = s->tallies.as<double>() + (size_t)r.slot * s->nbmax * nv;
+    int g = std::max(1, std::min((int)((nv + 255) / 256), e->sm_count * 8));
+    if (r.kind == 1) cudaMemsetAsync(s->f_dmax, 0, 8, st);
+    k_serve_finalize<<<g, 256, 0, st>>>(tal, r.nbatch, nv, scale, r.kind, e->mass_d.as<double>(),
+                                        e->rho_vox.as<double>(), (double)r.nper, s->f_dose, s->f_var, s->f_dmax);
+    if ((rc = cuda_check(e, cudaGetLastError(), "k_serve_finalize"))) return rc;
     if (r.kind == 0) {
-        if ((rc = finalize_dosxyz(e, s->f_sum, s->f_sum2, r.nbatch, (double)r.nper, s->f_dose, s->f_var))) return rc;
         r.dose.resize(nv);
         r.unc.resize(nv);
-        cudaMemcpyAsync(r.dose.data(), s->f_dose, nv * 8, cudaMemcpyDeviceToHost, e->stream);
-        cudaMemcpyAsync(r.unc.data(), s->f_var, nv * 8, cudaMemcpyDeviceToHost, e->stream);
-        return cuda_check(e, cudaStreamSynchronize(e->stream), "finalize beam request");
+        cudaMemcpyAsync(r.dose.data(), s->f_dose, nv * 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(r.unc.data(), s->f_var, nv * 8, cudaMemcpyDeviceToHost, st);
+        return cuda_check(e, cudaStreamSynchronize(st), "finalize beam request");
     }
-    if ((rc = finalize_matrad(e, s->f_sum, s->f_sum2, r.nbatch, s->f_dose, s->f_var))) return rc;
-    cudaMemsetAsync(s->f_dmax, 0, 8, e->stream);
-    int g = std::max(1, std::min((int)((nv + 255) / 256), e->sm_count * 4));
-    k_dmax<<<g, 256, 0, e->stream>>>(s->f_dose, nv, s->f_dmax);
     long seglen = (nv + NSEG - 1) / NSEG;
-    k_seg_count<<<NSEG, 256, 0, e->stream>>>(s->f_dose, nv, seglen, s->f_dmax, r.rel, s->f_cnt);
-    k_seg_scan<<<1, NSEG, 0, e->stream>>>(s->f_cnt, s->f_off, s->f_total);
-    k_seg_write<<<NSEG, 256, 0, e->stream>>>(s->f_dose, s->f_var, nv, seglen, s->f_dmax, r.rel, s->f_off, s->f_rows,
-                                              s->f_vals, s->f_vars, nv);
+    k_seg_count<<<NSEG, 256, 0, st>>>(s->f_dose, nv, seglen, s->f_dmax, r.rel, s->f_cnt);
+    k_seg_scan<<<1, NSEG, 0, st>>>(s->f_cnt, s->f_off, s->f_total);
+    k_seg_write<<<NSEG, 256, 0, st>>>(s->f_dose, s->f_var, nv, seglen, s->f_dmax, r.rel, s->f_off, s->f_rows,
+                                       s->f_vals, s->f_vars, nv);
     if ((rc = cuda_check(e, cudaGetLastError(), "sparse extraction"))) return rc;
     long long nnz = 0;
-    cudaMemcpyAsync(&nnz, s->f_total, 8, cudaMemcpyDeviceToHost, e->stream);
-    if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "sparse count"))) return rc;
+    cudaMemcpyAsync(&nnz, s->f_total, 8, cudaMemcpyDeviceToHost, st);
+    if ((rc = cuda_check(e, cudaStreamSynchronize(st), "sparse count"))) return rc;
     r.rows.resize(nnz);
     r.vals.resize(nnz);
     r.var.resize(nnz);
     if (nnz > 0) {
-        cudaMemcpyAsync(r.rows.data(), s->f_rows, nnz * 4, cudaMemcpyDeviceToHost, e->stream);
-        cudaMemcpyAsync(r.vals.data(), s->f_vals, nnz * 8, cudaMemcpyDeviceToHost, e->stream);
-        cudaMemcpyAsync(r.var.data(), s->f_vars, nnz * 8, cudaMemcpyDeviceToHost, e->stream);
+        cudaMemcpyAsync(r.rows.data(), s->f_rows, nnz * 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(r.vals.data(), s->f_vals, nnz * 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(r.var.data(), s->f_vars, nnz * 8, cudaMemcpyDeviceToHost, st);
     }
-    return cuda_check(e, cudaStreamSynchronize(e->stream), "sparse column");
+    return cuda_check(e, cudaStreamSynchronize(st), "sparse column");
 }
 
 int admit(omc_server *s) {
@@ -288,6 +389,7 @@ int admit(omc_server *s) {
         r.state = 1;
         s->injected = false;
         s->slot_req[slot] = r.id;
+        s->slot_seq[slot] = s->seq;
         s->order.push_back(slot);
         ServeReq q{};
         q.kind = r.kind;
@@ -312,10 +414,11 @@ int admit(omc_server *s) {
         changed = true;
     }
     if (changed) {
+        // pageable sources: the copies have taken the data when they return
         int n = (int)s->order.size();
         cudaMemcpyAsync(s->sd->order, s->order.data(), n * sizeof(int), cudaMemcpyHostToDevice, e->stream);
         cudaMemcpyAsync(&s->sd->norder, &n, sizeof(int), cudaMemcpyHostToDevice, e->stream);
-        return cuda_check(e, cudaStreamSynchronize(e->stream), "admission");
+        return cuda_check(e, cudaGetLastError(), "admission");
     }
     return OMC_OK;
 }
@@ -372,7 +475,29 @@ int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint6
     s->f_dmax = (unsigned long long *)(((uintptr_t)(s->f_off + NSEG) + 15) / 16 * 16);
     s->f_total = (long long *)(s->f_dmax + 1);
     s->slot_req.assign(s->nslots, -1);
+    s->slot_seq.assign(s->nslots, 0);
+    {
+        // pinned snapshot buffers, their events and the finalisation stream
+        size_t per = sizeof(ServeReq) * SERVE_MAX + sizeof(int) * SERVE_MAX + 64 + 8 * sizeof(int);
+        if (cudaHostAlloc(&s->snap_host, 2 * per, cudaHostAllocDefault) != cudaSuccess)
+            return set_err(e, OMC_E_CUDA, "server snapshot allocation failed");
+        for (int k = 0; k < 2; k++) {
+            char *b = (char *)s->snap_host + k * per;
+            s->snap[k].req = (ServeReq *)b;
+            s->snap[k].live = (int *)(b + sizeof(ServeReq) * SERVE_MAX);
+            s->snap[k].flags = (unsigned *)(b + sizeof(ServeReq) * SERVE_MAX + sizeof(int) * SERVE_MAX);
+            s->snap[k].qc = (int *)(b + sizeof(ServeReq) * SERVE_MAX + sizeof(int) * SERVE_MAX + 64);
+            if (cudaEventCreateWithFlags(&s->snap[k].ev, cudaEventDisableTiming) != cudaSuccess)
+                return set_err(e, OMC_E_CUDA, "server snapshot event");
+        }
+        if (cudaStreamCreateWithFlags(&s->fin_stream, cudaStreamNonBlocking) != cudaSuccess)
+            return set_err(e, OMC_E_CUDA, "server finalisation stream");
+    }
     s->target = std::min<long long>((long long)e->ev->cap / 2, e->ev->inflight);
+    {
+        int tail[2] = {SERVE_TAIL_PARTICLES, e->ev->boost};
+        cudaMemcpyAsync(&s->sd->tail_particles, tail, sizeof(tail), cudaMemcpyHostToDevice, e->stream);
+    }
     if (e->opt.profile) serve_profile_reset(e);
     // reset queue counters and capture two cycles as a graph
     Ctl c0{};
@@ -393,10 +518,6 @@ int omc_server_destroy(omc_server *s) {
     { std::lock_guard<std::mutex> lk(s->mu); }  // wait for a call in progress
     cudaSetDevice(s->e->device);
     cudaStreamSynchronize(s->e->stream);
-    if (s->exec) cudaGraphExecDestroy(s->exec);
-    if (s->graph) cudaGraphDestroy(s->graph);
-    if (s->t_start) cudaEventDestroy(s->t_start);
-    if (s->t_stop) cudaEventDestroy(s->t_stop);
     delete s;
     return OMC_OK;
 }
@@ -409,6 +530,21 @@ int omc_server_completed(omc_server *s, int *ids, int cap, int *n) {
     s->completed.erase(s->completed.begin(), s->completed.begin() + k);
     *n = k;
     return OMC_OK;
+}
+
+int omc_server_params(omc_server *s, int64_t tail_particles, int tail_boost) {
+    if (!s) return OMC_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    omc_engine *e = s->e;
+    cudaSetDevice(e->device);
+    if (tail_particles > (1LL << 30) || tail_boost > 1024)
+        return set_err(e, OMC_E_RANGE, "tail_particles at most 2^30, tail_boost at most 1024");
+    if (tail_particles >= 0) {
+        int v = (int)tail_particles;
+        cudaMemcpyAsync(&s->sd->tail_particles, &v, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+    }
+    if (tail_boost > 0) cudaMemcpyAsync(&s->sd->tail_boost, &tail_boost, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+    return cuda_check(e, cudaStreamSynchronize(e->stream), "server params");
 }
 
 int omc_server_stats(omc_server *s, double *out, int n) {
@@ -497,6 +633,71 @@ int omc_server_submit_beam(omc_server *s, const omc_beam *b, int64_t nhist, int 
     return submit(s, std::move(r), seed);
 }
 
+// Queue the snapshot of the request table, live counts, error flags and
+// queue counters after the work just queued.
+static int take_snapshot(omc_server *s) {
+    omc_engine *e = s->e;
+    omc_server::Snap &sn = s->snap[s->cur];
+    cudaMemcpyAsync(sn.req, s->sd->req, sizeof(ServeReq) * s->nslots, cudaMemcpyDeviceToHost, e->stream);
+    cudaMemcpyAsync(sn.live, s->sd->live, sizeof(int) * s->nslots, cudaMemcpyDeviceToHost, e->stream);
+    cudaMemcpyAsync(sn.flags, &e->ev->ctl_d->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream);
+    cudaMemcpyAsync(sn.qc, e->ev->ctl_d->cnt, 8 * sizeof(int), cudaMemcpyDeviceToHost, e->stream);
+    sn.seq = ++s->seq;
+    return cuda_check(e, cudaEventRecord(sn.ev, e->stream), "snapshot");
+}
+
+// Finish the requests that the snapshot shows complete (all histories
+// injected, no particle left) and admit pending ones into the freed slots.
+static int process_snapshot(omc_server *s, omc_server::Snap &sn) {
+    omc_engine *e = s->e;
+    int rc = cuda_check(e, cudaEventSynchronize(sn.ev), "server step");
+    if (rc) return rc;
+    if (*sn.flags & (ERR_QUEUE | ERR_NAN | ERR_STACK))
+        return set_err(e, OMC_E_DEVICE, "device error flags " + std::to_string(*sn.flags) + " in serving");
+    // a graph ends with a B -> A cycle: the particles are in queues A
+    const long long cap = e->ev->cap;
+    const int *qc = sn.qc;
+    s->left = std::min<long long>(qc[0] + qc[4], cap) + std::min<long long>(qc[1] + qc[5], cap);
+    if (sn.seq <= s->drain_seq) s->left = 0;   // taken before the drain emptied the queues
+    s->injected = true;
+    std::vector<int> keep;
+    bool freed = false;
+    for (int slot : s->order) {
+        Request &r = *s->reqs[s->slot_req[slot]];
+        if (sn.seq <= s->slot_seq[slot]) {   // admitted after this snapshot was taken
+            s->injected = false;
+            keep.push_back(slot);
+            continue;
+        }
+        const ServeReq &q = sn.req[slot];
+        if (q.next < r.nhist) s->injected = false;
+        if (q.next >= r.nhist && sn.live[slot] == 0) {
+            if ((rc = finalize_request(s, r))) return rc;
+            r.state = 2;
+            r.t_done = now_ms();
+            s->completed.push_back(r.id);
+            s->finished++;
+            s->slot_req[slot] = -1;
+            ServeReq fr{};
+            fr.kind = -1;
+            cudaMemcpyAsync(&s->sd->req[slot], &fr, sizeof(fr), cudaMemcpyHostToDevice, e->stream);
+            freed = true;
+        } else {
+            keep.push_back(slot);
+        }
+    }
+    sn.seq = 0;
+    if (freed) {
+        s->order = keep;
+        int n = (int)s->order.size();
+        if (n) cudaMemcpyAsync(s->sd->order, s->order.data(), n * sizeof(int), cudaMemcpyHostToDevice, e->stream);
+        cudaMemcpyAsync(&s->sd->norder, &n, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+        if ((rc = cuda_check(e, cudaGetLastError(), "server release"))) return rc;
+        if ((rc = admit(s))) return rc;
+    }
+    return OMC_OK;
+}
+
 int omc_server_step(omc_server *s, int cycles, int *active) {
     if (!s) return OMC_E_ARG;
     std::lock_guard<std::mutex> lk(s->mu);
@@ -504,13 +705,18 @@ int omc_server_step(omc_server *s, int cycles, int *active) {
     cudaSetDevice(e->device);
     int rc = admit(s);
     if (rc) return rc;
+    const int prev = s->cur ^ 1;
     if (!s->order.empty()) {
         const long long dthr = drain_threshold(e);
         const int per_cycle = e->d32.d.defer_interact ? 5 : 4;
         if (dthr > 0 && s->injected && s->pending.empty() && s->left > 0 && s->left <= dthr) {
+            // the drain's kernel reads the queue sizes on the device; `left`
+            // (from the last snapshot, taken before more cycles ran) bounds them
             serve_drain(e, s->sd, s->left, s->tallies.as<double>());
             s->drains++;
             s->launches++;
+            s->left = 0;
+            s->drain_seq = s->seq;
         } else if (e->opt.profile) {
             // cycles one by one, timed per kernel (the graph's two cycles)
             int graphs = std::max(1, cycles / 2);
@@ -525,50 +731,14 @@ int omc_server_step(omc_server *s, int cycles, int *active) {
             s->cycles += 2 * graphs;
             s->launches += 2 * graphs * per_cycle;
         }
-        // completion check: all injected and nothing left in the queues
-        std::vector<ServeReq> rq(s->nslots);
-        std::vector<int> live(s->nslots);
-        unsigned flags = 0;
-        int qc[8];  // Ctl::cnt, Ctl::cnt_hi
-        cudaMemcpyAsync(rq.data(), s->sd->req, sizeof(ServeReq) * s->nslots, cudaMemcpyDeviceToHost, e->stream);
-        cudaMemcpyAsync(live.data(), s->sd->live, sizeof(int) * s->nslots, cudaMemcpyDeviceToHost, e->stream);
-        cudaMemcpyAsync(&flags, &e->ev->ctl_d->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream);
-        cudaMemcpyAsync(qc, e->ev->ctl_d->cnt, sizeof(qc), cudaMemcpyDeviceToHost, e->stream);
-        if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "server step"))) return rc;
-        if (flags & (ERR_QUEUE | ERR_NAN | ERR_STACK))
-            return set_err(e, OMC_E_DEVICE, "device error flags " + std::to_string(flags) + " in serving");
-        // a graph ends with a B -> A cycle: the particles are in queues A
-        const long long cap = e->ev->cap;
-        s->left = std::min<long long>(qc[0] + qc[4], cap) + std::min<long long>(qc[1] + qc[5], cap);
-        s->injected = true;
-        std::vector<int> keep;
-        bool freed = false;
-        for (int slot : s->order) {
-            Request &r = *s->reqs[s->slot_req[slot]];
-            if (rq[slot].next < r.nhist) s->injected = false;
-            if (rq[slot].next >= r.nhist && live[slot] == 0) {
-                if ((rc = finalize_request(s, r))) return rc;
-                r.state = 2;
-                r.t_done = now_ms();
-                s->completed.push_back(r.id);
-                s->finished++;
-                s->slot_req[slot] = -1;
-                ServeReq q{};
-                q.kind = -1;
-                cudaMemcpyAsync(&s->sd->req[slot], &q, sizeof(q), cudaMemcpyHostToDevice, e->stream);
-                freed = true;
-            } else {
-                keep.push_back(slot);
-            }
-        }
-        if (freed) {
-            s->order = keep;
-            int n = (int)s->order.size();
-            if (n) cudaMemcpyAsync(s->sd->order, s->order.data(), n * sizeof(int), cudaMemcpyHostToDevice, e->stream);
-            cudaMemcpyAsync(&s->sd->norder, &n, sizeof(int), cudaMemcpyHostToDevice, e->stream);
-            if ((rc = cuda_check(e, cudaStreamSynchronize(e->stream), "server release"))) return rc;
-            if ((rc = admit(s))) return rc;
-        }
+        if ((rc = take_snapshot(s))) return rc;
+        s->cur ^= 1;
+    }
+    // the previous step's snapshot: ready once the work queued before it is
+    if (s->snap[prev].seq > 0 && (rc = process_snapshot(s, s->snap[prev]))) return rc;
+    if (s->order.empty() && s->snap[s->cur ^ 1].seq > 0) {
+        // nothing running: settle the snapshot just taken too
+        if ((rc = process_snapshot(s, s->snap[s->cur ^ 1]))) return rc;
     }
     if (active) *active = (int)(s->order.size() + s->pending.size());
     return OMC_OK;

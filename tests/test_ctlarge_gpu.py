@@ -1,0 +1,70 @@
+"""Dose parity on the full-size CT-like phantoms of the benchmark workloads,
+against the unmodified reference CLI (omc_dosxyz.c:1072-1307).
+
+tests/golden/refbig_<case>.npz (tests/golden/make_golden.py, make_big): one
+reference run per phantom, its dose and batch uncertainty in the voxels
+above 10 % of its maximum:
+  ct128  128x128x96 x 0.3 cm (the beamlet load's phantom), one 10x10 cm^2
+         beam of the 6 MV-like spectrum, 2.5e8 histories in 50 batches
+         (1.65 % mean relative uncertainty above 50 % of the maximum);
+  ct256  256x256x160 x 0.2 cm (10.5 M voxels), one 10x10 cm^2 beam of the
+         18 MV-like spectrum (pair and triplet production), 1.2e8 histories
+         in 40 batches.
+Both forms run the same beam: z = (D - D_ref) / sqrt(s^2 + s_ref^2) over
+those voxels, |z| < 3 in at least 99 % of them and mean z within 0.25."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RUNS = {
+    # case: (histories of the event form, histories of the plain form, batches)
+    "ct128": (250_000_000, 10_000_000, 20),
+    "ct256": (120_000_000, 5_000_000, 20),
+}
+
+_engines = {}
+
+
+def big_engine(case, assets_root):
+    from ompmc_b200 import assets as A
+    from ompmc_b200.engine import Engine, Tables
+    if case not in _engines:
+        for e in _engines.values():
+            e.close()
+        _engines.clear()
+        ph = A.ct_phantom(128, 128, 96, 0.3, seed=1234) if case == "ct128" else A.ct_phantom_large()
+        _engines[case] = Engine(Tables.from_assets(A.CT_MEDIA, assets_root), ph)
+    return _engines[case]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _release_engines():
+    yield
+    for e in _engines.values():
+        e.close()
+    _engines.clear()
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain_fp64", "event_fp32"])
+@pytest.mark.parametrize("case", sorted(RUNS))
+def test_large_phantom_dose_z(case, mode, golden, assets_root):
+    from ompmc_b200.engine import load_spectrum
+    g = golden(f"refbig_{case}")
+    eng = big_engine(case, assets_root)
+    spec = load_spectrum(assets_root / "spectra" / f"{str(g['spectrum'])}.spectrum")
+    n_event, n_plain, nbatch = RUNS[case]
+    dose, unc, st = eng.run_beam(n_event if mode == 1 else n_plain, nbatch, seed=2718 + mode, mode=mode,
+                                 spectrum=spec, collimator=tuple(g["collimator"]))
+    assert st["flags"] == 0
+    d = dose.ravel()[g["idx"]]
+    u = unc.ravel()[g["idx"]]
+    ref = g["dose"].astype(np.float64)
+    s = np.sqrt((u * d) ** 2 + (g["unc"] * ref) ** 2)
+    ok = s > 0
+    z = (d - ref)[ok] / s[ok]
+    frac = np.mean(np.abs(z) < 3)
+    print(f"{case} mode {mode}: {len(z)} voxels, |z|<3 in {frac:.4f}, mean z {z.mean():+.3f}, std {z.std():.3f}")
+    assert len(z) > 10000
+    assert frac >= 0.99, f"{case} mode {mode}: |z|<3 in {frac:.4f}; mean z {z.mean():.3f}"
+    assert abs(z.mean()) < 0.25, f"{case} mode {mode}: biased, mean z {z.mean():.3f}"

@@ -2,12 +2,14 @@
 tests/golden/dose*_<case>.npz, 50 batches): in voxels above 10 % of the
 reference maximum, z = (D_gpu - D_ref) / sqrt(s_gpu^2 + s_ref^2) with s the
 batch-method standard errors, |z| < 3 in >= 99 % of them and no systematic
-bias (mean z within 0.25), for the plain FP64 and the event FP32 forms.
+bias (mean z within 0.25), for the plain FP64 form and the event form in
+FP32 and in FP64 transport.
 Sources: the 6 MV-like spectrum on water, the slab and the 4-media CT-like
 phantom; the 18 MV-like spectrum on the slab (pair production in bone);
 6 MeV electron and 3 MeV positron beams on water (omc_dosxyz.c:596-605);
 the 6 MV-like spectrum with photon splitting (nsplit = 20) on water and the
-slab."""
+slab; the 6 MV-like spectrum on the slab and 6 MeV electrons on water with
+the synthetic spin file (spin rejection and moment corrections active)."""
 import numpy as np
 import pytest
 
@@ -16,7 +18,7 @@ from tests.conftest import CASES
 pytestmark = pytest.mark.gpu
 
 FIXTURES = ["dose_water30", "dose_slab64", "dose18_slab64", "dose_ctsmall", "dosee_water30", "dosep_water30",
-            "dosesplit_water30", "dosesplit_slab64"]
+            "dosesplit_water30", "dosesplit_slab64", "dosespin_slab64", "doseespin_water30"]
 
 
 def zscores(fixture, mode, golden, engine_for, assets_root, nbatch=50, seed=12345):
@@ -24,7 +26,8 @@ def zscores(fixture, mode, golden, engine_for, assets_root, nbatch=50, seed=1234
     g = golden(fixture)
     case = fixture.split("_", 1)[1]
     ns = int(g["nsplit"]) if "nsplit" in g else 1
-    eng = engine_for(case, nsplit=ns) if ns > 1 else engine_for(case)
+    data = str(g["spin_data"]) if "spin_data" in g else "data"
+    eng = engine_for(case, data=data, nsplit=ns) if ns > 1 else engine_for(case, data=data)
     spec_name = str(g["spectrum"]) if "spectrum" in g else "6mv"
     spec = load_spectrum(assets_root / "spectra" / f"{spec_name}.spectrum") if spec_name else None
     mono = float(g["mono_energy"]) if "mono_energy" in g else 1.25
@@ -40,8 +43,13 @@ def zscores(fixture, mode, golden, engine_for, assets_root, nbatch=50, seed=1234
     return z, st
 
 
-@pytest.mark.parametrize("mode", [0, 1], ids=["plain_fp64", "event_fp32"])
-@pytest.mark.parametrize("fixture", FIXTURES)
+# the FP64 event form (mode 2) has no photon splitting
+CASES_MODES = [pytest.param(f, m, id=f"{f}-{name}") for f in FIXTURES
+               for m, name in ((0, "plain_fp64"), (1, "event_fp32"), (2, "event_fp64"))
+               if not (m == 2 and f.startswith("dosesplit"))]
+
+
+@pytest.mark.parametrize("fixture,mode", CASES_MODES)
 def test_dose_z_scores(fixture, mode, golden, engine_for, assets_root):
     z, st = zscores(fixture, mode, golden, engine_for, assets_root)
     assert len(z) > 150
