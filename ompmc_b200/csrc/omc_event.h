@@ -57,13 +57,14 @@ struct Ctl {
     double src_energy;        // sum of primary kinetic energies
     int tsteps;               // this cycle's electron budget (tstep-loop iterations per event)
     float esplit;             // regroup energy (total, MeV): electrons above it go to the top
-    int fetch[3];             // work counters of the photon, electron and interaction kernels
-    int pad3;
+    int fetch[4];             // work counters of the photon, electron, interaction and tail kernels
     // counters per transport kernel (0 photon, 1 electron)
     unsigned long long st_events[2], st_steps[2], st_cross[2], st_dep[2], st_atom[2];
     // drain: the largest sub-history one thread ran (events, events of the
     // particle it started from, transport steps)
     int drain_max_events, drain_max_chain, drain_max_steps, drain_pad;
+    // serving: electrons of requests in their tail (tail queues A and B)
+    int cnt_tail[2], cnt_tail_hi[2];
 };
 
 // Per-kernel profile of the last run made with options.profile = 1.
@@ -90,8 +91,10 @@ struct EventStateT {
     DBuf buf[4];              // photon A, electron A, photon B, electron B (13 arrays each)
     DBuf split_buf[2];        // splitting state of the photon queues (nsplit > 1)
     DBuf int_buf;             // electrons at their discrete interaction (defer_interact)
+    DBuf tail_buf[2];         // serving: electrons of requests in their tail (A and B)
     QueueT<R> qi;
     QueueT<R> q[4];
+    QueueT<R> qt[2] = {};     // cap 0 until a server allocates them
     DBuf ctl;
     Ctl *ctl_d = nullptr;
     int block = 256;
@@ -165,6 +168,8 @@ int event_interact_queue(omc_engine *e);
 void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
 void serve_drain(omc_engine *e, ServeDev *sd, long long left, double *tallies);
 int serve_profiled_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
+// The tail queues of serving (allocated on first use).
+int event_tail_queues(omc_engine *e);
 void serve_profile_reset(omc_engine *e);
 // Particles left at or below which a run whose histories are all injected
 // switches from transport cycles to the drain kernel (0: never).

@@ -29,8 +29,11 @@
 namespace omc {
 // Default tail of a served request: once its histories are all injected and
 // at most this many of its particles are left, its electrons run with the
-// engine's tail_boost times the cycle's budget.
-constexpr int SERVE_TAIL_PARTICLES = 4096;
+// engine's tail_boost times the cycle's budget.  Off: measured on the served
+// beamlet load, boosted lanes share warps with unboosted ones and stall them
+// (saturated throughput 27.4 M hist/s off, 14.2 at 4096 particles, 10.9 at
+// 16384), for a p99 at 70 % load that improves only with the lower load.
+constexpr int SERVE_TAIL_PARTICLES = 0;
 int finalize_dosxyz(omc_engine *e, const double *sum, const double *sum2, int nbatch, double nper, double *dose,
                     double *unc);
 int finalize_matrad(omc_engine *e, const double *sum, const double *sum2, int nbatch, double *dose, double *var);
@@ -294,7 +297,7 @@ struct omc_server {
         ServeReq *req = nullptr;
         int *live = nullptr;
         unsigned *flags = nullptr;
-        int *qc = nullptr;     // Ctl::cnt, Ctl::cnt_hi
+        int *qc = nullptr;     // Ctl::cnt, Ctl::cnt_hi, then Ctl::cnt_tail, Ctl::cnt_tail_hi
         cudaEvent_t ev = nullptr;
         long long seq = 0;     // 0: none pending
     } snap[2];
@@ -433,6 +436,7 @@ int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint6
     cudaSetDevice(e->device);
     int rc = event_prepare(e);
     if (!rc) rc = event_interact_queue(e);
+    if (!rc) rc = event_tail_queues(e);
     if (rc) return rc;
     auto s = std::make_unique<omc_server>();
     s->e = e;
@@ -478,7 +482,7 @@ int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint6
     s->slot_seq.assign(s->nslots, 0);
     {
         // pinned snapshot buffers, their events and the finalisation stream
-        size_t per = sizeof(ServeReq) * SERVE_MAX + sizeof(int) * SERVE_MAX + 64 + 8 * sizeof(int);
+        size_t per = sizeof(ServeReq) * SERVE_MAX + sizeof(int) * SERVE_MAX + 64 + 12 * sizeof(int);
         if (cudaHostAlloc(&s->snap_host, 2 * per, cudaHostAllocDefault) != cudaSuccess)
             return set_err(e, OMC_E_CUDA, "server snapshot allocation failed");
         for (int k = 0; k < 2; k++) {
@@ -642,6 +646,7 @@ static int take_snapshot(omc_server *s) {
     cudaMemcpyAsync(sn.live, s->sd->live, sizeof(int) * s->nslots, cudaMemcpyDeviceToHost, e->stream);
     cudaMemcpyAsync(sn.flags, &e->ev->ctl_d->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream);
     cudaMemcpyAsync(sn.qc, e->ev->ctl_d->cnt, 8 * sizeof(int), cudaMemcpyDeviceToHost, e->stream);
+    cudaMemcpyAsync(sn.qc + 8, e->ev->ctl_d->cnt_tail, 4 * sizeof(int), cudaMemcpyDeviceToHost, e->stream);
     sn.seq = ++s->seq;
     return cuda_check(e, cudaEventRecord(sn.ev, e->stream), "snapshot");
 }
@@ -657,7 +662,8 @@ static int process_snapshot(omc_server *s, omc_server::Snap &sn) {
     // a graph ends with a B -> A cycle: the particles are in queues A
     const long long cap = e->ev->cap;
     const int *qc = sn.qc;
-    s->left = std::min<long long>(qc[0] + qc[4], cap) + std::min<long long>(qc[1] + qc[5], cap);
+    s->left = std::min<long long>(qc[0] + qc[4], cap) + std::min<long long>(qc[1] + qc[5], cap) +
+              std::min<long long>(qc[8] + qc[10], e->ev->qt[0].cap);
     if (sn.seq <= s->drain_seq) s->left = 0;   // taken before the drain emptied the queues
     s->injected = true;
     std::vector<int> keep;

@@ -369,6 +369,32 @@ def make_big(name, cores=8):
                         loop_seconds=loop_s, cores=cores, spectrum=spectrum, collimator=np.array([-5, 5, -5, 5.0]))
 
 
+# high-statistics reference doses of the BIG cases for the gamma test
+GAMMA_BIG = {"ct128": (1_000_000_000, 100)}
+
+
+def make_gamma_big(name, cores=8):
+    """Reference CLI dose of a BIG case at GAMMA_BIG's histories ->
+    gammabig_<name>.npz (voxels above 10 % of the maximum, float32)."""
+    from oracle.ref import run_cli
+    mk, spectrum, _, _ = BIG[name]
+    ncase, nbatch = GAMMA_BIG[name]
+    A.require_assets()
+    pf = WORK / f"{name}.egsphant"
+    if not pf.exists():
+        A.write_egsphant(pf, mk())
+    run = A.default_run(pf, spectrum=spectrum, ncase=ncase, nbatch=nbatch, collimator=(-5, 5, -5, 5))
+    base = WORK / f"gammabig_{name}_{ncase}"
+    A.write_inp(base, run)
+    loop_s, _ = run_cli(base, f"gammabig_{name}", cores=cores, timeout=12 * 3600)
+    dose, unc, _ = A.read_3ddose(A.ASSETS / "out" / f"gammabig_{name}.3ddose")
+    keep = np.flatnonzero(dose.ravel() > 0.1 * dose.max())
+    np.savez_compressed(HERE / f"gammabig_{name}.npz", idx=keep.astype(np.int32),
+                        dose=dose.ravel()[keep].astype(np.float32), unc=unc.ravel()[keep].astype(np.float32),
+                        shape=np.array(dose.shape), dmax=dose.max(), ncase=ncase, nbatch=nbatch,
+                        loop_seconds=loop_s, cores=cores, spectrum=spectrum, collimator=np.array([-5, 5, -5, 5.0]))
+
+
 DIJ = dict(gantry=[0.0, 90.0], bixel=1.0, field=(2.0, 2.0), nhist=100000, nbatch=10, rel=1e-4)
 
 
@@ -432,6 +458,11 @@ def main():
             continue
         print("generating refbig", name, flush=True)
         make_big(name, cores=a.cores)
+    for name in GAMMA_BIG:
+        if a.only and a.only not in f"gammabig_{name}":
+            continue
+        print("generating gammabig", name, flush=True)
+        make_gamma_big(name, cores=a.cores)
     if not a.only or a.only in "dij_ctsmall":
         print("generating dij_ctsmall", flush=True)
         make_dij()
