@@ -315,16 +315,6 @@ int omc_server_timer(omc_server *s, int stop, double *ms);
  * by one with events around each kernel, and omc_profile_last reports the
  * per-kernel times and transport counters of everything it has run. */
 int omc_server_stats(omc_server *s, double *out, int n);
-/* Tail budget of a server's requests (no reference counterpart): once a
- * request's histories are all injected and at most tail_particles of its
- * particles are left, its electrons get tail_boost (default: the engine's
- * tail_boost option) times the cycle's budget of tstep-loop iterations per
- * event, so its longest chains finish in fewer cycles.  tail_particles 0
- * (the default) turns it off: the boosted lanes stall the warps they share,
- * which costs more throughput than it saves latency under load.  A negative
- * value, or tail_boost <= 0, keeps the current value.  Results do not
- * depend on it. */
-int omc_server_params(omc_server *s, int64_t tail_particles, int tail_boost);
 
 /* ---------------------------------------------- drop-in CLI (dosxyz)
  * The whole omc_dosxyz program (omc_dosxyz.c:1072-1307): reads

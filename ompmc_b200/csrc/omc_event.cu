@@ -52,7 +52,7 @@ constexpr int electron_minb() {
 
 template <typename R>
 using TransportKernelT = void (*)(DevData<R>, QueueT<R>, QueueT<R>, QueueT<R>, double *, long, Ctl *, uint32_t,
-                                  ServeDev *, int, QueueT<R>, QueueT<R>);
+                                  ServeDev *, int, QueueT<R>);
 using TransportKernel = TransportKernelT<float>;
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -245,7 +245,7 @@ template <int MAXOUT, bool DEFER = false, typename R = float>
 __device__ __forceinline__ int emit(const QueueT<R> &outP, const QueueT<R> &outE, bool alive, const Part<R> &p,
                                     EvEnv<MAXOUT, R> &g, int slot, uint32_t k0, uint32_t k1, float esplit,
                                     int sp = -1, float sr = 0.f, const QueueT<R> *outI = nullptr,
-                                    bool defer = false, const QueueT<R> *outT = nullptr, bool tail = false) {
+                                    bool defer = false) {
     const unsigned full = 0xffffffffu;
     uint64_t pkey = ((uint64_t)k1 << 32) | k0;
     int queued = 0;
@@ -278,19 +278,11 @@ __device__ __forceinline__ int emit(const QueueT<R> &outP, const QueueT<R> &outE
         const bool toi = DEFER && k == 0 && defer;
         bool isph = has && q.iq == 0 && !toi;
         bool isel = has && q.iq != 0 && !toi;
-        // electrons of a request in its tail go to the tail queue (serving)
-        const bool ist = outT && isel && tail;
-        isel = isel && !ist;
         int ip = warp_append(outP, isph, false, full, g.flags);
         int ie = warp_append(outE, isel, esplit > 0.f && q.e > (R)esplit, full, g.flags);
         if (ip >= 0) qstore(outP, ip, q, slot, a0, a1, ac, k == 0 ? sp : -1, k == 0 ? sr : 0.f);
         if (ie >= 0) qstore(outE, ie, q, slot, a0, a1, ac);
         queued += (ip >= 0) + (ie >= 0);
-        if (outT) {
-            int it = warp_append(*outT, ist, false, full, g.flags);
-            if (it >= 0) qstore(*outT, it, q, slot, a0, a1, ac);
-            queued += it >= 0;
-        }
         if (DEFER && k == 0) {
             int ii = warp_append(*outI, has && toi, false, full, g.flags);
             if (ii >= 0) qstore(*outI, ii, q, slot, a0, a1, ac);
@@ -391,15 +383,14 @@ __device__ __forceinline__ bool split_event(const DevData<R> &D, Env &g, Part<R>
 // D.defer_interact).  `qi`: the interaction queue (EV_ELECTRON with
 // D.defer_interact appends there).
 enum { EV_PHOTON = 0, EV_ELECTRON = 1, EV_SPLIT = 2, EV_INTERACT = 3, EV_ELECTRON_DEFER = 4 };
-template <int KIND, typename R = float, bool TAIL = false>
+template <int KIND, typename R = float>
 __device__ __forceinline__ void transport_events(const DevData<R> &D, const QueueT<R> &in, const QueueT<R> &outP,
                                                  const QueueT<R> &outE, double *tallies, long nvox, Ctl *ctl,
-                                                 uint32_t seedw, ServeDev *sd, int nbmax, const QueueT<R> &qi,
-                                                 const QueueT<R> &qt) {
+                                                 uint32_t seedw, ServeDev *sd, int nbmax, const QueueT<R> &qi) {
     constexpr int MAXOUT = KIND == EV_SPLIT ? EV_MAXOUT_SPLIT : EV_MAXOUT;
     const unsigned full = 0xffffffffu;
     constexpr bool ELECTRON = KIND == EV_ELECTRON || KIND == EV_ELECTRON_DEFER;
-    const int kq = TAIL ? 3 : (ELECTRON ? 1 : (KIND == EV_INTERACT ? 2 : 0));
+    const int kq = ELECTRON ? 1 : (KIND == EV_INTERACT ? 2 : 0);
     const int ks = KIND == EV_PHOTON || KIND == EV_SPLIT ? 0 : 1;   // counters: photon or electron
     const int n = queue_size(in);
     const int tsteps = ctl->tsteps;
@@ -433,9 +424,7 @@ __device__ __forceinline__ void transport_events(const DevData<R> &D, const Queu
         g.nout = 0;
         g.flags = 0;
         g.work = 0;
-        // the tail kernel (TAIL) runs its electrons with the request's boost
-        const bool tail = sd && valid && sd->boost[slot / nbmax] > 1;
-        g.tleft = TAIL && tail ? tsteps * sd->boost[slot / nbmax] : tsteps;
+        g.tleft = tsteps;
         g.ncross = g.ndep = g.natom = 0;
         bool alive = false, defer = false;
         if (valid) {
@@ -453,12 +442,9 @@ __device__ __forceinline__ void transport_events(const DevData<R> &D, const Queu
             }
             g.flush();
         }
-        const QueueT<R> *outT = qt.cap > 0 ? &qt : nullptr;
         int emitted = KIND == EV_ELECTRON_DEFER
-                          ? emit<MAXOUT, true, R>(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr, &qi, defer,
-                                                  outT, tail)
-                          : emit<MAXOUT, false, R>(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr, nullptr,
-                                                   false, outT, tail);
+                          ? emit<MAXOUT, true, R>(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr, &qi, defer)
+                          : emit<MAXOUT, false, R>(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr);
         if (sd) add_live(sd->live, nbmax, valid ? slot : 0, valid ? emitted - 1 : 0, full);
         flags |= g.flags;
         c_ev += valid;
@@ -480,29 +466,27 @@ __device__ __forceinline__ void transport_events(const DevData<R> &D, const Queu
 template <typename R>
 __global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_step(DevData<R> D, QueueT<R> in, QueueT<R> outP,
                                                      QueueT<R> outE, double *tallies, long nvox, Ctl *ctl,
-                                                     uint32_t seedw, ServeDev *sd, int nbmax, QueueT<R> qi,
-                                                     QueueT<R> qt) {
-    transport_events<EV_PHOTON, R>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd, nbmax, qi, qt);
+                                                     uint32_t seedw, ServeDev *sd, int nbmax, QueueT<R> qi) {
+    transport_events<EV_PHOTON, R>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd, nbmax, qi);
 }
 
 // Photon events of a splitting engine (nsplit > 1): one sub-photon each.
 __global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_split_step(DevData<float> D, Queue in, Queue outP,
                                                            Queue outE, double *tallies, long nvox, Ctl *ctl,
-                                                           uint32_t seedw, ServeDev *sd, int nbmax, Queue qi,
-                                                           Queue qt) {
-    transport_events<EV_SPLIT>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd, nbmax, qi, qt);
+                                                           uint32_t seedw, ServeDev *sd, int nbmax, Queue qi) {
+    transport_events<EV_SPLIT>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd, nbmax, qi);
 }
 
 // Electron/positron events of the queued charged particles: at most the
 // cycle's budget of tstep-loop iterations each, then the particle is
 // re-queued.  The step is latency bound; the occupancy it is compiled for
 // (electron_minb) trades resident warps against spilled local frames.
-template <bool DEFER, typename R = float, bool TAIL = false>
+template <bool DEFER, typename R = float>
 __global__ void __launch_bounds__(EV_MAX_BLOCK, electron_minb<R>())
     k_electron_step(DevData<R> D, QueueT<R> in, QueueT<R> outP, QueueT<R> outE, double *tallies, long nvox, Ctl *ctl,
-                    uint32_t seedw, ServeDev *sd, int nbmax, QueueT<R> qi, QueueT<R> qt) {
-    transport_events<DEFER ? EV_ELECTRON_DEFER : EV_ELECTRON, R, TAIL>(D, in, outP, outE, tallies, nvox, ctl, seedw,
-                                                                        sd, nbmax, qi, qt);
+                    uint32_t seedw, ServeDev *sd, int nbmax, QueueT<R> qi) {
+    transport_events<DEFER ? EV_ELECTRON_DEFER : EV_ELECTRON, R>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd,
+                                                                  nbmax, qi);
 }
 
 // The electron kernel of the engine: interactions in a kernel of their own
@@ -518,9 +502,8 @@ static TransportKernelT<R> electron_kernel(const omc_engine *e) {
 template <typename R = float>
 __global__ void __launch_bounds__(EV_MAX_BLOCK) k_electron_interact(DevData<R> D, QueueT<R> in, QueueT<R> outP,
                                                            QueueT<R> outE, double *tallies, long nvox, Ctl *ctl,
-                                                           uint32_t seedw, ServeDev *sd, int nbmax, QueueT<R> qi,
-                                                           QueueT<R> qt) {
-    transport_events<EV_INTERACT, R>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd, nbmax, qi, qt);
+                                                           uint32_t seedw, ServeDev *sd, int nbmax, QueueT<R> qi) {
+    transport_events<EV_INTERACT, R>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd, nbmax, qi);
 }
 
 // ------------------------------------------------------------ drain
@@ -554,19 +537,19 @@ struct DrainPart {
 
 // STATS (profiled runs): record the largest sub-history a thread ran.
 template <bool SPLIT, bool STATS = false, typename R = float>
-__global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<R> D, QueueT<R> qP, QueueT<R> qE, QueueT<R> qT,
-                                                        double *tallies, long nvox, Ctl *ctl, uint32_t seedw) {
+__global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<R> D, QueueT<R> qP, QueueT<R> qE, double *tallies,
+                                                        long nvox, Ctl *ctl, uint32_t seedw) {
     constexpr int MAXOUT = SPLIT ? EV_MAXOUT_SPLIT : EV_MAXOUT;
-    const int np = queue_size(qP), ne = queue_size(qE), nt = qT.cap > 0 ? queue_size(qT) : 0;
-    const int n = np + ne + nt;
+    const int np = queue_size(qP), ne = queue_size(qE);
+    const int n = np + ne;
     DrainPart<R> st[DRAIN_STACK];
     unsigned flags = 0;
     unsigned long long c_ev[2] = {0, 0}, c_steps[2] = {0, 0}, c_cross[2] = {0, 0}, c_dep[2] = {0, 0},
                        c_atom[2] = {0, 0};
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const QueueT<R> &q = t < np ? qP : (t < np + ne ? qE : qT);
+        const QueueT<R> &q = t < np ? qP : qE;
         int tag = 0;
-        const int qi = queue_index(q, t < np ? t : (t < np + ne ? t - np : t - np - ne));
+        const int qi = queue_index(q, t < np ? t : t - np);
         qload(q, qi, st[0].p, tag, st[0].k0, st[0].k1, st[0].pos);
         st[0].sp = (SPLIT && q.sp) ? q.sp[qi] : -1;
         st[0].sr = (SPLIT && q.sr) ? q.sr[qi] : 0.f;
@@ -706,7 +689,6 @@ __device__ __forceinline__ void plan_budget(Ctl *ctl, long long nE, const PlanCf
     ctl->fetch[0] = 0;
     ctl->fetch[1] = 0;
     ctl->fetch[2] = 0;
-    ctl->fetch[3] = 0;
     ctl->cnt_int = 0;
     ctl->cnt_int_hi = 0;
 }
@@ -724,8 +706,6 @@ __device__ __forceinline__ void plan_queues(Ctl *ctl, int iph, int iel, int cap,
     ctl->cnt[iel ^ 2] = 0;
     ctl->cnt_hi[iph ^ 2] = 0;
     ctl->cnt_hi[iel ^ 2] = 0;
-    ctl->cnt_tail[(iph ^ 2) >> 1] = 0;
-    ctl->cnt_tail_hi[(iph ^ 2) >> 1] = 0;
 }
 
 // Histories to inject this cycle: keep `target` particles in flight (a
@@ -833,19 +813,6 @@ static void size_grids(omc_engine *e, EventStateT<R> &S) {
     S.lanes = S.grid_e * S.block;
 }
 
-// The tail queues of serving (FP32), allocated when a server first needs
-// them: a quarter of the main queues' capacity each.
-int event_tail_queues(omc_engine *e) {
-    EventState &S = *e->ev;
-    if (S.tail_buf[0].p) return OMC_OK;
-    for (int k = 0; k < 2; k++) {
-        int rc = alloc_queue(e, S.tail_buf[k], S.qt[k], std::max(1024, S.cap / 4), &S.ctl_d->cnt_tail[k],
-                             &S.ctl_d->cnt_tail_hi[k]);
-        if (rc) return rc;
-    }
-    return OMC_OK;
-}
-
 // The interaction queue, allocated when the engine first needs it.
 template <typename R>
 static int event_interact_queue_t(omc_engine *e) {
@@ -913,30 +880,19 @@ static void launch_transport(omc_engine *e, int iph, int iel, int oph, int oel, 
     EventStateT<R> &S = *state_of<R>(e);
     const long nvox = e->ph.nvox();
     const DevData<R> D = event_data<R>(e);
-    // serving: the tail queue this cycle reads (tin) and the one it fills
-    const int tin = iph >> 1, tout = oph >> 1;
-    const QueueT<R> qto = S.qt[tout];
     auto photons = [&](cudaStream_t st) {
         photon_kernel<R>(e)<<<S.grid_p, S.block, 0, st>>>(D, S.q[iph], S.q[oph], S.q[oel], tallies, nvox, S.ctl_d,
-                                                          seedw, sd, nbmax, S.qi, qto);
-    };
-    // electrons of requests in their tail, with the request's larger budget
-    // and interactions in place: their own warps, beside the photons
-    auto tail = [&](cudaStream_t st) {
-        if (sd && S.qt[tin].cap > 0)
-            k_electron_step<false, R, true><<<e->sm_count, S.block, 0, st>>>(
-                D, S.qt[tin], S.q[oph], S.q[oel], tallies, nvox, S.ctl_d, seedw, sd, nbmax, S.qi, qto);
+                                                          seedw, sd, nbmax, S.qi);
     };
     auto electrons = [&]() {
         electron_kernel<R>(e)<<<S.grid_e, S.block, 0, e->stream>>>(D, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
-                                                                    S.ctl_d, seedw, sd, nbmax, S.qi, qto);
+                                                                    S.ctl_d, seedw, sd, nbmax, S.qi);
         if (D.defer_interact)
             k_electron_interact<R><<<S.grid_i, S.block, 0, e->stream>>>(D, S.qi, S.q[oph], S.q[oel], tallies, nvox,
-                                                                        S.ctl_d, seedw, sd, nbmax, S.qi, qto);
+                                                                        S.ctl_d, seedw, sd, nbmax, S.qi);
     };
     if (ev || !S.side) {
         photons(e->stream);
-        tail(e->stream);
         if (ev) cudaEventRecord(ev[3], e->stream);
         electrons();
         return;
@@ -945,7 +901,6 @@ static void launch_transport(omc_engine *e, int iph, int iel, int oph, int oel, 
     cudaStreamWaitEvent(S.side, S.fork, 0);
     electrons();
     photons(S.side);
-    tail(S.side);
     cudaEventRecord(S.join, S.side);
     cudaStreamWaitEvent(e->stream, S.join, 0);
 }
@@ -1042,14 +997,13 @@ static void launch_drain(omc_engine *e, int iph, long long left, double *tallies
     long long g = (left + DRAIN_BLOCK - 1) / DRAIN_BLOCK;
     g = std::max(1LL, std::min(g, (long long)S.drain_lanes / DRAIN_BLOCK * 4));
     const DevData<R> D = event_data<R>(e);
-    void (*kd)(DevData<R>, QueueT<R>, QueueT<R>, QueueT<R>, double *, long, Ctl *, uint32_t);
+    void (*kd)(DevData<R>, QueueT<R>, QueueT<R>, double *, long, Ctl *, uint32_t);
     if constexpr (sizeof(R) == 4)
         kd = D.nsplit > 1 ? (stats ? k_drain<true, true, R> : k_drain<true, false, R>)
                           : (stats ? k_drain<false, true, R> : k_drain<false, false, R>);
     else
         kd = stats ? k_drain<false, true, R> : k_drain<false, false, R>;
-    kd<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(D, S.q[iph], S.q[iph + 1], S.qt[iph >> 1], tallies, e->ph.nvox(),
-                                              S.ctl_d, seedw);
+    kd<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(D, S.q[iph], S.q[iph + 1], tallies, e->ph.nvox(), S.ctl_d, seedw);
 }
 
 // Profiled transport: cycles launched one by one with events around each
@@ -1325,11 +1279,6 @@ __global__ void __launch_bounds__(SERVE_MAX) k_serve_plan(ServeDev *sd, Ctl *ctl
         sd->plan_cum[pos] = (int)before;
         sd->req[slot].next = next + take;
     }
-    if (slot >= 0) {
-        // the tail of a request whose histories are all in: a larger budget
-        const bool tail = rem == take && sd->tail_particles > 0 && sd->live[slot] <= sd->tail_particles;
-        sd->boost[slot] = tail ? sd->tail_boost : 1;
-    }
     // the last thread sees the totals
     if (k == blockDim.x - 1) {
         const long long total_rem = before + rem;
@@ -1439,8 +1388,6 @@ void serve_drain(omc_engine *e, ServeDev *sd, long long left, double *tallies) {
     cudaMemsetAsync(sd->live, 0, sizeof(sd->live), e->stream);
     cudaMemsetAsync(S.ctl_d->cnt, 0, 2 * sizeof(int), e->stream);
     cudaMemsetAsync(S.ctl_d->cnt_hi, 0, 2 * sizeof(int), e->stream);
-    cudaMemsetAsync(&S.ctl_d->cnt_tail[0], 0, sizeof(int), e->stream);
-    cudaMemsetAsync(&S.ctl_d->cnt_tail_hi[0], 0, sizeof(int), e->stream);
 }
 
 }  // namespace omc

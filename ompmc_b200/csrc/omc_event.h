@@ -57,14 +57,13 @@ struct Ctl {
     double src_energy;        // sum of primary kinetic energies
     int tsteps;               // this cycle's electron budget (tstep-loop iterations per event)
     float esplit;             // regroup energy (total, MeV): electrons above it go to the top
-    int fetch[4];             // work counters of the photon, electron, interaction and tail kernels
+    int fetch[3];             // work counters of the photon, electron and interaction kernels
+    int pad3;
     // counters per transport kernel (0 photon, 1 electron)
     unsigned long long st_events[2], st_steps[2], st_cross[2], st_dep[2], st_atom[2];
     // drain: the largest sub-history one thread ran (events, events of the
     // particle it started from, transport steps)
     int drain_max_events, drain_max_chain, drain_max_steps, drain_pad;
-    // serving: electrons of requests in their tail (tail queues A and B)
-    int cnt_tail[2], cnt_tail_hi[2];
 };
 
 // Per-kernel profile of the last run made with options.profile = 1.
@@ -91,10 +90,8 @@ struct EventStateT {
     DBuf buf[4];              // photon A, electron A, photon B, electron B (13 arrays each)
     DBuf split_buf[2];        // splitting state of the photon queues (nsplit > 1)
     DBuf int_buf;             // electrons at their discrete interaction (defer_interact)
-    DBuf tail_buf[2];         // serving: electrons of requests in their tail (A and B)
     QueueT<R> qi;
     QueueT<R> q[4];
-    QueueT<R> qt[2] = {};     // cap 0 until a server allocates them
     DBuf ctl;
     Ctl *ctl_d = nullptr;
     int block = 256;
@@ -144,18 +141,11 @@ struct ServeDev {
     BeamSrc<float> beam[SERVE_MAX];
     BeamletSrc<float> bl[SERVE_MAX];
     int live[SERVE_MAX];       // particles of the request in the queues
-    int boost[SERVE_MAX];      // electron budget multiplier of the request's particles this cycle
     int order[SERVE_MAX];      // active slots in admission order
     int norder;
     int nplan;
     int inject_total;
     int pad;
-    // a request whose histories are all injected and which has at most
-    // tail_particles particles left runs them with tail_boost times the
-    // cycle's electron budget (0: never), so its longest chains take fewer
-    // cycles; budgets do not change trajectories
-    int tail_particles;
-    int tail_boost;
     int plan_slot[SERVE_MAX];
     long long plan_first[SERVE_MAX];
     int plan_cum[SERVE_MAX + 1];
@@ -168,8 +158,6 @@ int event_interact_queue(omc_engine *e);
 void serve_launch_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
 void serve_drain(omc_engine *e, ServeDev *sd, long long left, double *tallies);
 int serve_profiled_cycle(omc_engine *e, int in, ServeDev *sd, double *tallies, int nbmax, long long target);
-// The tail queues of serving (allocated on first use).
-int event_tail_queues(omc_engine *e);
 void serve_profile_reset(omc_engine *e);
 // Particles left at or below which a run whose histories are all injected
 // switches from transport cycles to the drain kernel (0: never).

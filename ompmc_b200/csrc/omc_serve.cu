@@ -27,13 +27,6 @@
 #include "omc_source.cuh"
 
 namespace omc {
-// Default tail of a served request: once its histories are all injected and
-// at most this many of its particles are left, its electrons run with the
-// engine's tail_boost times the cycle's budget.  Off: measured on the served
-// beamlet load, boosted lanes share warps with unboosted ones and stall them
-// (saturated throughput 27.4 M hist/s off, 14.2 at 4096 particles, 10.9 at
-// 16384), for a p99 at 70 % load that improves only with the lower load.
-constexpr int SERVE_TAIL_PARTICLES = 0;
 int finalize_dosxyz(omc_engine *e, const double *sum, const double *sum2, int nbatch, double nper, double *dose,
                     double *unc);
 int finalize_matrad(omc_engine *e, const double *sum, const double *sum2, int nbatch, double *dose, double *var);
@@ -128,18 +121,31 @@ __global__ void k_seg_write(const double *d, const double *v, long n, long segle
 // dose with its uncertainty (dosxyz, accumulateResults omc_dosxyz.c:719-799)
 // or variance of the mean (matRad, omc_matrad.c:920-1012) is written.
 // HBM traffic: nbatch tallies read and zeroed, two outputs written.
+// All of a voxel's batch values are loaded before any is zeroed, so a
+// thread has up to NB loads in flight (loads and stores of the same array
+// would otherwise be issued one after the other); streaming hints, since
+// every value is touched once.
+template <int NB>
 __global__ void k_serve_finalize(double *__restrict__ tal, int nbatch, long nv, double scale, int kind,
                                  const double *__restrict__ mass, const double *__restrict__ rho, double nper,
                                  double *__restrict__ dose, double *__restrict__ second,
                                  unsigned long long *dmaxbits) {
     double m = 0.0;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nv; i += (long)gridDim.x * blockDim.x) {
+        double x[NB];
+#pragma unroll
+        for (int b = 0; b < NB; b++) x[b] = b < nbatch ? __ldcs(&tal[(size_t)b * nv + i]) : 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; b++)
+            if (b < nbatch) __stcs(&tal[(size_t)b * nv + i], 0.0);
         double sum = 0.0, sum2 = 0.0;
-        for (int b = 0; b < nbatch; b++) {
-            double x = tal[(size_t)b * nv + i] * scale;
-            sum += x;
-            sum2 += x * x;
-            tal[(size_t)b * nv + i] = 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            if (b < nbatch) {
+                const double v = x[b] * scale;
+                sum += v;
+                sum2 += v * v;
+            }
         }
         double en, u;
         if (kind == 0) {
@@ -177,8 +183,8 @@ __global__ void k_serve_finalize(double *__restrict__ tal, int nbatch, long nv, 
             }
             m = fmax(m, en);
         }
-        dose[i] = en;
-        second[i] = u;
+        __stcs(&dose[i], en);
+        __stcs(&second[i], u);
     }
     if (kind != 0) {
         for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
@@ -266,13 +272,15 @@ struct Request {
 
 }  // namespace
 
+constexpr int SERVE_NBMAX = 10;   // batches of a served request, at most
+
 struct omc_server {
     // Guards everything below: submissions may come from any host thread
     // while one thread steps the server (a matRad-side producer beside the
     // driving loop); every omc_server_* call holds it for its duration.
     std::mutex mu;
     omc_engine *e = nullptr;
-    int nbmax = 10, nslots = 0;
+    int nbmax = SERVE_NBMAX, nslots = 0;
     long long target = 0;
     uint64_t seed = 0;
     DBuf tallies, sdbuf, fin;
@@ -297,7 +305,7 @@ struct omc_server {
         ServeReq *req = nullptr;
         int *live = nullptr;
         unsigned *flags = nullptr;
-        int *qc = nullptr;     // Ctl::cnt, Ctl::cnt_hi, then Ctl::cnt_tail, Ctl::cnt_tail_hi
+        int *qc = nullptr;     // Ctl::cnt, Ctl::cnt_hi
         cudaEvent_t ev = nullptr;
         long long seq = 0;     // 0: none pending
     } snap[2];
@@ -348,8 +356,10 @@ int finalize_request(omc_server *s, Request &r) {
     double *tal = s->tallies.as<double>() + (size_t)r.slot * s->nbmax * nv;
     int g = std::max(1, std::min((int)((nv + 255) / 256), e->sm_count * 8));
     if (r.kind == 1) cudaMemsetAsync(s->f_dmax, 0, 8, st);
-    k_serve_finalize<<<g, 256, 0, st>>>(tal, r.nbatch, nv, scale, r.kind, e->mass_d.as<double>(),
-                                        e->rho_vox.as<double>(), (double)r.nper, s->f_dose, s->f_var, s->f_dmax);
+    static_assert(SERVE_NBMAX == 10, "k_serve_finalize is instantiated for the server's batch limit");
+    k_serve_finalize<SERVE_NBMAX><<<g, 256, 0, st>>>(tal, r.nbatch, nv, scale, r.kind, e->mass_d.as<double>(),
+                                                     e->rho_vox.as<double>(), (double)r.nper, s->f_dose, s->f_var,
+                                                     s->f_dmax);
     if ((rc = cuda_check(e, cudaGetLastError(), "k_serve_finalize"))) return rc;
     if (r.kind == 0) {
         r.dose.resize(nv);
@@ -436,7 +446,6 @@ int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint6
     cudaSetDevice(e->device);
     int rc = event_prepare(e);
     if (!rc) rc = event_interact_queue(e);
-    if (!rc) rc = event_tail_queues(e);
     if (rc) return rc;
     auto s = std::make_unique<omc_server>();
     s->e = e;
@@ -482,7 +491,7 @@ int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint6
     s->slot_seq.assign(s->nslots, 0);
     {
         // pinned snapshot buffers, their events and the finalisation stream
-        size_t per = sizeof(ServeReq) * SERVE_MAX + sizeof(int) * SERVE_MAX + 64 + 12 * sizeof(int);
+        size_t per = sizeof(ServeReq) * SERVE_MAX + sizeof(int) * SERVE_MAX + 64 + 8 * sizeof(int);
         if (cudaHostAlloc(&s->snap_host, 2 * per, cudaHostAllocDefault) != cudaSuccess)
             return set_err(e, OMC_E_CUDA, "server snapshot allocation failed");
         for (int k = 0; k < 2; k++) {
@@ -498,10 +507,6 @@ int omc_server_create(omc_engine *e, int64_t mem_budget, int max_requests, uint6
             return set_err(e, OMC_E_CUDA, "server finalisation stream");
     }
     s->target = std::min<long long>((long long)e->ev->cap / 2, e->ev->inflight);
-    {
-        int tail[2] = {SERVE_TAIL_PARTICLES, e->ev->boost};
-        cudaMemcpyAsync(&s->sd->tail_particles, tail, sizeof(tail), cudaMemcpyHostToDevice, e->stream);
-    }
     if (e->opt.profile) serve_profile_reset(e);
     // reset queue counters and capture two cycles as a graph
     Ctl c0{};
@@ -534,21 +539,6 @@ int omc_server_completed(omc_server *s, int *ids, int cap, int *n) {
     s->completed.erase(s->completed.begin(), s->completed.begin() + k);
     *n = k;
     return OMC_OK;
-}
-
-int omc_server_params(omc_server *s, int64_t tail_particles, int tail_boost) {
-    if (!s) return OMC_E_ARG;
-    std::lock_guard<std::mutex> lk(s->mu);
-    omc_engine *e = s->e;
-    cudaSetDevice(e->device);
-    if (tail_particles > (1LL << 30) || tail_boost > 1024)
-        return set_err(e, OMC_E_RANGE, "tail_particles at most 2^30, tail_boost at most 1024");
-    if (tail_particles >= 0) {
-        int v = (int)tail_particles;
-        cudaMemcpyAsync(&s->sd->tail_particles, &v, sizeof(int), cudaMemcpyHostToDevice, e->stream);
-    }
-    if (tail_boost > 0) cudaMemcpyAsync(&s->sd->tail_boost, &tail_boost, sizeof(int), cudaMemcpyHostToDevice, e->stream);
-    return cuda_check(e, cudaStreamSynchronize(e->stream), "server params");
 }
 
 int omc_server_stats(omc_server *s, double *out, int n) {
@@ -646,7 +636,6 @@ static int take_snapshot(omc_server *s) {
     cudaMemcpyAsync(sn.live, s->sd->live, sizeof(int) * s->nslots, cudaMemcpyDeviceToHost, e->stream);
     cudaMemcpyAsync(sn.flags, &e->ev->ctl_d->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream);
     cudaMemcpyAsync(sn.qc, e->ev->ctl_d->cnt, 8 * sizeof(int), cudaMemcpyDeviceToHost, e->stream);
-    cudaMemcpyAsync(sn.qc + 8, e->ev->ctl_d->cnt_tail, 4 * sizeof(int), cudaMemcpyDeviceToHost, e->stream);
     sn.seq = ++s->seq;
     return cuda_check(e, cudaEventRecord(sn.ev, e->stream), "snapshot");
 }
@@ -662,8 +651,7 @@ static int process_snapshot(omc_server *s, omc_server::Snap &sn) {
     // a graph ends with a B -> A cycle: the particles are in queues A
     const long long cap = e->ev->cap;
     const int *qc = sn.qc;
-    s->left = std::min<long long>(qc[0] + qc[4], cap) + std::min<long long>(qc[1] + qc[5], cap) +
-              std::min<long long>(qc[8] + qc[10], e->ev->qt[0].cap);
+    s->left = std::min<long long>(qc[0] + qc[4], cap) + std::min<long long>(qc[1] + qc[5], cap);
     if (sn.seq <= s->drain_seq) s->left = 0;   // taken before the drain emptied the queues
     s->injected = true;
     std::vector<int> keep;

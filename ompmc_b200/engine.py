@@ -126,7 +126,6 @@ def lib():
         "omc_server_completed": ([C.c_void_p, _ip, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "omc_server_timer": ([C.c_void_p, C.c_int, _dp], C.c_int),
         "omc_server_stats": ([C.c_void_p, _dp, C.c_int], C.c_int),
-        "omc_server_params": ([C.c_void_p, C.c_int64, C.c_int], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name, None)
@@ -534,10 +533,6 @@ class Server:
         n = C.c_int()
         _check(lib().omc_server_completed(self.h, _p(ids, _ip), int(cap), C.byref(n)), self.engine.h)
         return ids[:n.value].tolist()
-
-    def params(self, tail_particles=-1, tail_boost=0):
-        """Tail budget of the requests (omc_server_params)."""
-        _check(lib().omc_server_params(self.h, int(tail_particles), int(tail_boost)), self.engine.h)
 
     def stats(self):
         """Cycles, drains, kernel launches and finished requests so far."""

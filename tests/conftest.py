@@ -50,6 +50,15 @@ def case_phantom(name):
     raise KeyError(name)
 
 
+def z_outliers_allowed(n):
+    """Voxels that may lie beyond |z| = 3 in a z-test over n voxels: 1 % of
+    them, or for small n the 99.9 % Poisson quantile of the count expected
+    when z follows a Student t of about 50 degrees of freedom (0.5 % of the
+    voxels), whichever is larger."""
+    from scipy.stats import poisson
+    return max(int(0.01 * n), int(poisson.ppf(0.999, 0.005 * n)))
+
+
 _engines = {}
 
 

@@ -1,9 +1,11 @@
 """Statistical dose parity with the reference CPU code (omc_dosxyz CLI,
 tests/golden/dose*_<case>.npz, 50 batches): in voxels above 10 % of the
 reference maximum, z = (D_gpu - D_ref) / sqrt(s_gpu^2 + s_ref^2) with s the
-batch-method standard errors, |z| < 3 in >= 99 % of them and no systematic
-bias (mean z within 0.25), for the plain FP64 form and the event form in
-FP32 and in FP64 transport.
+batch-method standard errors, |z| < 3 in >= 99 % of them (for fixtures with
+few such voxels, the count beyond 3 at most the 99.9 % Poisson quantile of
+what a t distribution gives: tests.conftest.z_outliers_allowed) and no
+systematic bias (mean z within 0.25), for the plain FP64 form and the event
+form in FP32 and in FP64 transport.
 Sources: the 6 MV-like spectrum on water, the slab and the 4-media CT-like
 phantom; the 18 MV-like spectrum on the slab (pair production in bone);
 6 MeV electron and 3 MeV positron beams on water (omc_dosxyz.c:596-605);
@@ -51,10 +53,12 @@ CASES_MODES = [pytest.param(f, m, id=f"{f}-{name}") for f in FIXTURES
 
 @pytest.mark.parametrize("fixture,mode", CASES_MODES)
 def test_dose_z_scores(fixture, mode, golden, engine_for, assets_root):
+    from tests.conftest import z_outliers_allowed
     z, st = zscores(fixture, mode, golden, engine_for, assets_root)
     assert len(z) > 150
     frac = np.mean(np.abs(z) < 3)
-    assert frac >= 0.99, f"{fixture} mode {mode}: |z|<3 in {frac:.4f}; mean z {z.mean():.3f}"
+    nbad = int(np.sum(np.abs(z) >= 3))
+    assert nbad <= z_outliers_allowed(len(z)), f"{fixture} mode {mode}: |z|<3 in {frac:.4f}; mean z {z.mean():.3f}"
     assert abs(z.mean()) < 0.25, f"{fixture} mode {mode}: biased, mean z {z.mean():.3f}"
 
 

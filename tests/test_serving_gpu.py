@@ -5,8 +5,7 @@
   summation order of the tally atomics may differ, rtol 1e-9);
 * the drain (the last particles run to the end in one launch once every
   admitted history is injected) changes no result: the same request with
-  the drain off gives the same column; nor does the tail budget of a
-  request's last particles;
+  the drain off gives the same column;
 * submissions from two producer threads while a third steps the server;
 * admission by memory: with a budget for two requests, eight requests all
   finish, first come first served, with results identical to an unbounded
@@ -84,31 +83,6 @@ def test_drain_changes_no_result(engine_for, assets_root):
     assert np.array_equal(a[0], b[0])
     np.testing.assert_allclose(b[1], a[1], rtol=1e-9)
     np.testing.assert_allclose(b[2], a[2], rtol=1e-6, atol=1e-40)
-
-
-def test_tail_budget_changes_no_result(engine_for, assets_root):
-    """The tail budget (a request's last particles run with a larger
-    electron budget per cycle) changes no result: tail off, default and a
-    tail covering the whole request give the same column."""
-    from ompmc_b200.engine import Server, load_spectrum
-    eng = engine_for("ctsmall")
-    bl = bixels(engine_for)
-    bl["spectrum"] = load_spectrum(assets_root / "spectra" / "6mv.spectrum")
-    out = []
-    for tail in (0, -1, 1 << 30):                 # off, default, always
-        srv = Server(eng, seed=5)
-        srv.params(tail_particles=tail)
-        bs = srv.beamlet_set(bl)
-        ids = {k: srv.submit_beamlet(bs, k, 20000, 10, 1e-4, seed=900 + k) for k in (2, 9)}
-        out.append(run_all(srv, ids))
-        srv.close()
-    for k in (2, 9):
-        a = out[0][k]
-        assert len(a[0]) > 100
-        for b in out[1:]:
-            assert np.array_equal(a[0], b[k][0])
-            np.testing.assert_allclose(b[k][1], a[1], rtol=1e-9)
-            np.testing.assert_allclose(b[k][2], a[2], rtol=1e-6, atol=1e-40)
 
 
 def test_admission_by_memory_budget(engine_for, assets_root):
