@@ -72,3 +72,27 @@ def test_large_phantom_dose_z(case, mode, golden, assets_root):
     assert len(z) > 10000
     assert frac >= 0.99, f"{case} mode {mode}: |z|<3 in {frac:.4f}; mean z {z.mean():.3f}"
     assert abs(z.mean()) < 0.25, f"{case} mode {mode}: biased, mean z {z.mean():.3f}"
+
+
+def test_large_phantom_gamma_event_form(golden, assets_root):
+    """Gamma 2 %/2 mm of the FP32 event form against the reference CLI at
+    10^9 histories on the 128x128x96 phantom (tests/golden/gammabig_ct128.npz,
+    0.8 % mean relative uncertainty above 50 % of its maximum); the event
+    form runs twice the reference's histories so that its own noise is the
+    smaller part.  Global criterion normalised to the reference maximum:
+    gamma <= 1 in at least 99 % of the voxels above 10 % of it."""
+    from ompmc_b200 import assets as A
+    from ompmc_b200.engine import EVENT_FP32, load_spectrum
+    from ompmc_b200.gamma import gamma_pass_rate
+    g = golden("gammabig_ct128")
+    eng = big_engine("ct128", assets_root)
+    ph = A.ct_phantom(128, 128, 96, 0.3, seed=1234)
+    spec = load_spectrum(assets_root / "spectra" / f"{str(g['spectrum'])}.spectrum")
+    d, u, st = eng.run_beam(2 * int(g["ncase"]), 10, seed=4711, mode=EVENT_FP32, spectrum=spec,
+                            collimator=tuple(g["collimator"]))
+    assert st["flags"] == 0
+    rate, gam = gamma_pass_rate(g["idx"], g["dose"].astype(np.float64), d, (ph.xb, ph.yb, ph.zb), dd=0.02, dta=0.2,
+                                cutoff=0.1, d_norm=float(g["dmax"]))
+    print(f"ct128 gamma 2%/2mm: {rate:.4f} over {len(gam)} voxels")
+    assert len(gam) > 10000
+    assert rate >= 0.99, f"gamma 2%/2mm pass rate {rate:.4f}"
