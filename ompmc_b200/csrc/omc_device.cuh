@@ -89,9 +89,6 @@ struct DevData {
     const PL<R> *pmax;               // [nmed*MXGE]
     const Rayl<R> *ray;              // [nmed]
     const ElBin<R> *el;              // [(nmed*2)*MXEKE]: (imed*2+qel)*MXEKE + bin
-#if OMC_EL_SMEM
-    int el_stride;                   // bins between (medium, charge) rows of `el`
-#endif
     const MsE<R> *msurf;             // [NMS]
     const R *spin;                   // [nmed][2][32][16][32]
     R b2spin_min, dbeta2i, espml, dleneri, dqq1i, dllambi, dqmsi;

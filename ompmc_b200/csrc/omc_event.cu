@@ -481,30 +481,6 @@ __global__ void __launch_bounds__(EV_MAX_BLOCK) k_photon_split_step(DevData<floa
 // cycle's budget of tstep-loop iterations each, then the particle is
 // re-queued.  The step is latency bound; the occupancy it is compiled for
 // (electron_minb) trades resident warps against spilled local frames.
-#if OMC_EL_SMEM
-// Experiment: the electron bins of the media in play staged in shared memory
-// per block (rows of EL_SMEM_ROW bins), at the occupancy that leaves.
-constexpr int EL_SMEM_ROW = 150;
-template <bool DEFER, typename R = float>
-__global__ void __launch_bounds__(EV_MAX_BLOCK, 2)
-    k_electron_step(DevData<R> D, QueueT<R> in, QueueT<R> outP, QueueT<R> outE, double *tallies, long nvox, Ctl *ctl,
-                    uint32_t seedw, ServeDev *sd, int nbmax, QueueT<R> qi) {
-    extern __shared__ __align__(16) unsigned char el_smem[];
-    ElBin<R> *sh = (ElBin<R> *)el_smem;
-    const int rows = D.nmed * 2;
-    for (int k = threadIdx.x; k < rows * EL_SMEM_ROW; k += blockDim.x)
-        sh[k] = D.el[(k / EL_SMEM_ROW) * D_MXEKE + k % EL_SMEM_ROW];
-    __syncthreads();
-    DevData<R> Dl = D;
-    Dl.el = sh;
-    Dl.el_stride = EL_SMEM_ROW;
-    transport_events<DEFER ? EV_ELECTRON_DEFER : EV_ELECTRON, R>(Dl, in, outP, outE, tallies, nvox, ctl, seedw, sd,
-                                                                  nbmax, qi);
-}
-static size_t el_smem_bytes(const omc_engine *e) {
-    return (size_t)e->d32.d.nmed * 2 * EL_SMEM_ROW * sizeof(ElBin<float>);
-}
-#else
 template <bool DEFER, typename R = float>
 __global__ void __launch_bounds__(EV_MAX_BLOCK, electron_minb<R>())
     k_electron_step(DevData<R> D, QueueT<R> in, QueueT<R> outP, QueueT<R> outE, double *tallies, long nvox, Ctl *ctl,
@@ -512,8 +488,6 @@ __global__ void __launch_bounds__(EV_MAX_BLOCK, electron_minb<R>())
     transport_events<DEFER ? EV_ELECTRON_DEFER : EV_ELECTRON, R>(D, in, outP, outE, tallies, nvox, ctl, seedw, sd,
                                                                   nbmax, qi);
 }
-static size_t el_smem_bytes(const omc_engine *) { return 0; }
-#endif
 
 // The electron kernel of the engine: interactions in a kernel of their own
 // (D.defer_interact) or in place.
@@ -828,12 +802,7 @@ template <typename R>
 static void size_grids(omc_engine *e, EventStateT<R> &S) {
     int bp = 0, be = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, photon_kernel<R>(e), S.block, 0);
-    const size_t esm = sizeof(R) == 4 ? el_smem_bytes(e) : 0;
-    if (esm) {
-        cudaFuncSetAttribute(k_electron_step<true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esm);
-        cudaFuncSetAttribute(k_electron_step<false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esm);
-    }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, electron_kernel<R>(e), S.block, esm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&be, electron_kernel<R>(e), S.block, 0);
     S.grid_p = e->sm_count * std::max(1, bp);
     S.grid_e = e->sm_count * std::max(1, be);
     int bi = 0, bd = 0;
@@ -909,16 +878,15 @@ template <typename R = float>
 static void launch_transport(omc_engine *e, int iph, int iel, int oph, int oel, double *tallies, uint32_t seedw,
                              ServeDev *sd, int nbmax, cudaEvent_t *ev) {
     EventStateT<R> &S = *state_of<R>(e);
-    // the kernels use it as the distance between consecutive tally slots
-    const long nvox = sd && S.tally_stride > 0 ? S.tally_stride : e->ph.nvox();
+    const long nvox = e->ph.nvox();
     const DevData<R> D = event_data<R>(e);
     auto photons = [&](cudaStream_t st) {
         photon_kernel<R>(e)<<<S.grid_p, S.block, 0, st>>>(D, S.q[iph], S.q[oph], S.q[oel], tallies, nvox, S.ctl_d,
                                                           seedw, sd, nbmax, S.qi);
     };
     auto electrons = [&]() {
-        electron_kernel<R>(e)<<<S.grid_e, S.block, sizeof(R) == 4 ? el_smem_bytes(e) : 0, e->stream>>>(
-            D, S.q[iel], S.q[oph], S.q[oel], tallies, nvox, S.ctl_d, seedw, sd, nbmax, S.qi);
+        electron_kernel<R>(e)<<<S.grid_e, S.block, 0, e->stream>>>(D, S.q[iel], S.q[oph], S.q[oel], tallies, nvox,
+                                                                    S.ctl_d, seedw, sd, nbmax, S.qi);
         if (D.defer_interact)
             k_electron_interact<R><<<S.grid_i, S.block, 0, e->stream>>>(D, S.qi, S.q[oph], S.q[oel], tallies, nvox,
                                                                         S.ctl_d, seedw, sd, nbmax, S.qi);
@@ -1024,7 +992,7 @@ long long drain_threshold(const omc_engine *e) { return drain_threshold_t<float>
 // records its largest sub-history.
 template <typename R = float>
 static void launch_drain(omc_engine *e, int iph, long long left, double *tallies, uint32_t seedw,
-                         bool stats = false, long stride = 0) {
+                         bool stats = false) {
     EventStateT<R> &S = *state_of<R>(e);
     long long g = (left + DRAIN_BLOCK - 1) / DRAIN_BLOCK;
     g = std::max(1LL, std::min(g, (long long)S.drain_lanes / DRAIN_BLOCK * 4));
@@ -1035,8 +1003,7 @@ static void launch_drain(omc_engine *e, int iph, long long left, double *tallies
                           : (stats ? k_drain<false, true, R> : k_drain<false, false, R>);
     else
         kd = stats ? k_drain<false, true, R> : k_drain<false, false, R>;
-    kd<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(D, S.q[iph], S.q[iph + 1], tallies, stride > 0 ? stride : e->ph.nvox(),
-                                              S.ctl_d, seedw);
+    kd<<<(int)g, DRAIN_BLOCK, 0, e->stream>>>(D, S.q[iph], S.q[iph + 1], tallies, e->ph.nvox(), S.ctl_d, seedw);
 }
 
 // Profiled transport: cycles launched one by one with events around each
@@ -1417,7 +1384,7 @@ void serve_profile_reset(omc_engine *e) {
 // queues are emptied and every request's live count is zero.
 void serve_drain(omc_engine *e, ServeDev *sd, long long left, double *tallies) {
     EventState &S = *e->ev;
-    launch_drain(e, 0, left, tallies, SERVE_SEEDW, false, S.tally_stride);
+    launch_drain(e, 0, left, tallies, SERVE_SEEDW);
     cudaMemsetAsync(sd->live, 0, sizeof(sd->live), e->stream);
     cudaMemsetAsync(S.ctl_d->cnt, 0, 2 * sizeof(int), e->stream);
     cudaMemsetAsync(S.ctl_d->cnt_hi, 0, 2 * sizeof(int), e->stream);

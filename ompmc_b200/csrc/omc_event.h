@@ -103,7 +103,6 @@ struct EventStateT {
     int tsteps = 2;           // electron tstep iterations per event launch
     double esplit = 0;        // regroup energy of the electron queues (total, MeV)
     long long inflight = 0;   // particles kept in flight by the injector
-    long tally_stride = 0;    // serving: doubles between consecutive batch tallies (0: the voxel count)
     KernelProfile prof[4];    // 0 source, 1 photon, 2 electron, 3 plan+reset
     // profiled runs: per cycle {histories injected, photons in, electrons in,
     // source ms, photon ms, electron ms}

@@ -102,11 +102,7 @@ template <typename R>
 OMC_HD const ElBin<R> &ebin(const DevData<R> &D, int imed, int qel, int l) {
     int meke = D.ms[imed].meke;
     l = l < 0 ? 0 : (l >= meke ? meke - 1 : l);
-#if OMC_EL_SMEM
-    return D.el[(imed * 2 + qel) * D.el_stride + l];
-#else
     return D.el[(imed * 2 + qel) * D_MXEKE + l];
-#endif
 }
 template <typename R>
 OMC_HD const PhBin<R> &pbin(const DevData<R> &D, int imed, int l) {

@@ -91,7 +91,7 @@ def test_admission_by_memory_budget(engine_for, assets_root):
     bl = bixels(engine_for)
     bl["spectrum"] = load_spectrum(assets_root / "spectra" / "6mv.spectrum")
     nvox = int(np.prod(eng.shape))
-    per_req = 10 * ((nvox + 31) // 32 * 32 + 32) * 8     # ten batch tallies at the server's padded stride
+    per_req = 10 * nvox * 8
     results = []
     for budget in (2 * per_req + 100, 0):
         s = Server(eng, mem_budget=budget, seed=3)
