@@ -163,18 +163,28 @@ def atomic_peak(device, n_vox):
     return n * reps / (s.elapsed_time(e) * 1e-3)
 
 
-def ncu_traffic_per_event():
-    """DRAM bytes per electron event from the committed ncu summary."""
-    p = REPO / "profiles" / "electron_transport_slab64.md"
+PROFILE_SLAB = "electron_transport_slab64.md"
+PROFILE_REQUESTS = "electron_requests_beamlets_ct128.md"
+
+
+def ncu_figure(name, key):
+    """A per-event figure (`key: value` line) of a committed ncu summary."""
+    p = REPO / "profiles" / name
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
-        if line.strip().startswith("dram_bytes_per_event:"):
+        if line.strip().startswith(key + ":"):
             try:
                 return float(line.split(":")[1].split()[0])
             except ValueError:
                 return None
     return None
+
+
+def ncu_traffic_per_event():
+    """DRAM bytes per electron event from the committed ncu summary of the
+    slab case."""
+    return ncu_figure(PROFILE_SLAB, "dram_bytes_per_event")
 
 
 def reference_rate(root, ph, spec_path, ncase, cores):
@@ -452,12 +462,12 @@ def unc_summary(unc, nhist, rate):
             "seconds_to_1pct_per_beamlet": float(np.mean(q) / 1e-4 / rate), "beamlets": int(ok.sum())}
 
 
-def beamlet_engine(load, device, profile=False):
+def beamlet_engine(load, device, profile=False, queue_capacity=0):
     from ompmc_b200.engine import Engine, Tables, load_spectrum
     from ompmc_b200 import assets as A
     load["spectrum"] = load_spectrum(load["spectrum_file"])
     eng = Engine(Tables.from_assets(load["media"], A.require_assets()), load["phantom"], ecut=0.7, pcut=0.01,
-                 device=device, profile=profile)
+                 device=device, profile=profile, queue_capacity=queue_capacity)
     return eng
 
 
@@ -521,6 +531,12 @@ def main_beamlets(args):
                                      "served_hist_per_s": lp["histories"] / lp["wall_s"],
                                      "p50_ms": float(np.percentile(lp["lat_ms"], 50)),
                                      "p99_ms": float(np.percentile(lp["lat_ms"], 99))}
+        # one request at a time, the reference's mode, on the beamlets of the
+        # CPU baseline's sample
+        sl, srate = serve_sequential(srv, load, args.ref_beamlets, seed0 + 7000)
+        extras["sequential"] = {"requests": args.ref_beamlets, "p50_ms": float(np.percentile(sl, 50)),
+                                "p99_ms": float(np.percentile(sl, 99)), "hist_per_s": srate,
+                                "mode": "each request submitted when the previous column is in host memory"}
     srv.close()
     if rank == 0 and not args.no_extras and world == 1:
         extras.update(beamlet_extras(args, load, eng, value, local))
@@ -561,32 +577,35 @@ def beamlet_extras(args, load, eng, value, device):
     peak, peak_kind = peaks()
     # a profiled pass over part of the load: per-kernel device time and
     # transport counters with the kernels launched one by one
-    pe = beamlet_engine(load, device, profile=True)
-    ps = Server(pe, seed=99)
-    sub = np.arange(min(args.profile_requests, len(load["order"])))
-    serve_load(ps, load, args.arrival_rate, 424242, idx=sub)
-    prof = pe.profile_last()
-    ps.close()
-    pe.close()
+    prof, hist, nsub = profiled_pass(load, device, args.profile_requests, args.arrival_rate)
     ek, pk = prof["electron"], prof["photon"]
-    lookups = 10 * ek["steps"] + 3 * ek["particles"]
-    alg_bytes = 8 * ek["cross"] + 16 * ek["dep"] + 8 * lookups
+    nl = max(1, ek["launches"])
+    # table and voxel bytes the electron kernels request per event, counted
+    # by ncu's SASS counters on this load (queue state excluded); the
+    # code-read estimate of 10 table pair lookups per condensed-history step
+    # + 3 per event is kept beside it
+    req = ncu_figure(PROFILE_REQUESTS, "requested_bytes_per_event")
+    est_bytes = 8 * ek["cross"] + 16 * ek["dep"] + 8 * (10 * ek["steps"] + 3 * ek["particles"])
+    alg_bytes = (req - 104) * ek["particles"] if req else est_bytes
     achieved = alg_bytes / ek["seconds"] / 1e9
-    tpe = ncu_traffic_per_event()
-    per_launch_events = ek["particles"] / max(1, ek["launches"])
+    tpe = ncu_figure(PROFILE_REQUESTS, "dram_bytes_per_event") or ncu_traffic_per_event()
+    per_launch_events = ek["particles"] / nl
     total_s = sum(x["seconds"] for x in prof.values())
     extras["roofline"] = {
         "bound": "hbm", "kernel": "k_electron_step + k_electron_interact (+ k_drain)", "achieved": achieved,
         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
         "traffic": (tpe * per_launch_events) if tpe else None,
-        "algorithmic_bytes_per_launch": alg_bytes / max(1, ek["launches"]),
+        "algorithmic_bytes_per_launch": alg_bytes / nl,
+        "algorithmic_bytes": "requested by the kernels' global loads, stores and reductions (ncu SASS counters, "
+                             "per event) less the 104 B of queue state" if req else
+                             "8 B per voxel crossing + 16 B per deposit + 8 B per estimated table pair lookup",
+        "estimated_bytes_per_launch": est_bytes / nl,
         "state_bytes_per_launch": 104 * per_launch_events,
-        "avg_launch_ms": 1000 * ek["seconds"] / max(1, ek["launches"]),
+        "avg_launch_ms": 1000 * ek["seconds"] / nl,
         "kernel_seconds": {k: v["seconds"] for k, v in prof.items()},
         "kernel_share": {k: v["seconds"] / max(1e-12, total_s) for k, v in prof.items()},
-        "sample": f"profiled pass over {len(sub)} requests of the load",
+        "sample": f"profiled pass over {nsub} requests of the load",
     }
-    hist = float(np.sum(load["nhist"][sub]))
     extras["per_history"] = {k: (ek[k] + pk[k]) / hist for k in ("particles", "steps", "cross", "dep", "atom")}
     # plain FP64 history-based form on a sample of the same beamlets, one
     # after the other (omc_run_beamlets)
@@ -620,6 +639,53 @@ def beamlet_extras(args, load, eng, value, device):
     else:
         extras["cpu_baseline"] = None
     return extras
+
+
+def profiled_pass(load, device, nreq, rate, max_requests=0, queue_capacity=0):
+    """The first `nreq` requests of the load through a server whose engine
+    launches every kernel on its own with events around it and counts
+    transport events (particles), condensed-history steps, voxel crossings,
+    deposits and tally atomics per kernel.  Returns those counters, the
+    histories of the pass and the request count."""
+    from ompmc_b200.engine import Server
+    pe = beamlet_engine(load, device, profile=True, queue_capacity=queue_capacity)
+    ps = Server(pe, seed=99, max_requests=max_requests)
+    sub = np.arange(min(nreq, len(load["order"])))
+    serve_load(ps, load, rate, 424242, idx=sub)
+    prof = pe.profile_last()
+    ps.close()
+    pe.close()
+    return prof, float(np.sum(load["nhist"][sub])), len(sub)
+
+
+def serve_sequential(srv, load, n, seed, cycles=4):
+    """The first `n` requests of the load served one at a time, the way the
+    reference's matRad entry runs its beamlets: each request is submitted
+    once the previous one's sparse column is in host memory.  Returns the
+    latency of each request (ms, submission to column in host memory) and
+    the histories/s of the sequence."""
+    from ompmc_b200.workloads import LOAD_NBATCH, LOAD_REL
+    bs = srv.beamlet_set(dict(load["beamlets"], spectrum=load["spectrum"]))
+    lat = []
+    t_all = time.perf_counter()
+    for k in range(n):
+        b = int(load["order"][k])
+        t0 = time.perf_counter()
+        srv.submit_beamlet(bs, b, int(load["nhist"][k]), LOAD_NBATCH, LOAD_REL, seed=seed * 100003 + b + 1)
+        done = False
+        for guard in range(10_000_000):
+            srv.step(cycles)
+            for rid in srv.completed():
+                srv.result_sparse(rid)
+                srv.release(rid)
+                done = True
+            if done:
+                break
+        else:
+            raise RuntimeError("sequential request did not finish")
+        lat.append(1e3 * (time.perf_counter() - t0))
+    wall = time.perf_counter() - t_all
+    return np.array(lat), float(np.sum(load["nhist"][:n])) / wall
 
 
 def ref_summary(res):
@@ -905,7 +971,21 @@ def main():
     ap.add_argument("--serving-params", default=None,
                     help="event-form parameters of the serving engine (and of the --cycle-trace run), as JSON "
                          "(Engine.event_params keywords)")
+    ap.add_argument("--profiled-pass", action="store_true",
+                    help="beamlets: run only the profiled pass over --profile-requests requests (the case of the "
+                         "ncu capture of the electron kernel's requested bytes) and print its counters")
+    ap.add_argument("--profile-max-requests", type=int, default=0,
+                    help="profiled pass: requests resident at once (0: as the memory budget allows)")
+    ap.add_argument("--profile-queue-capacity", type=int, default=0,
+                    help="profiled pass: particle queue capacity (0: the engine's default)")
     args = ap.parse_args()
+    if args.profiled_pass:
+        from ompmc_b200.workloads import beamlet_load
+        prof, hist, nsub = profiled_pass(beamlet_load(args.load_seed), int(os.environ.get("LOCAL_RANK", "0")),
+                                         args.profile_requests, args.arrival_rate, args.profile_max_requests,
+                                         args.profile_queue_capacity)
+        print(json.dumps({"requests": nsub, "histories": hist, "counters": prof}))
+        return 0
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "slab64" or args.serving_only or args.cycle_trace:

@@ -102,11 +102,11 @@ typedef struct {
     double electron_split; /* event form: electrons above this kinetic energy
                              (MeV) are queued apart from the others so that
                              warps see particles of one kind (0 = one group,
-                             default 0.3); results do not depend on it */
+                             default 0.15); results do not depend on it */
     int electron_chsteps; /* event form: condensed-history steps after which an
                              electron's distance to its next discrete
                              interaction is drawn afresh (memoryless, so the
-                             sampled physics is the same; default 2; 0 = the
+                             sampled physics is the same; default 3; 0 = the
                              reference's restart after every step, which
                              also costs a zero-length step each time) */
     int electron_interact_kernel; /* event form: 1 (default) = electrons'

@@ -35,13 +35,13 @@ SPACE = {
     "tail_boost": [1, 8, 32, 128],
     "inflight": [1 << 18, 1 << 19, 1 << 20, 1 << 21],
     "block": [64, 128, 256],
-    "electron_split": [0.0, 0.2, 0.3, 0.5, 1.0],
-    "electron_chsteps": [1, 2, 4, 8],
+    "electron_split": [0.0, 0.1, 0.15, 0.2, 0.3, 0.5, 1.0],
+    "electron_chsteps": [1, 2, 3, 4, 8],
     "drain_particles": [-1, 10000, 20000, 40000, 80000],
 }
 # the starting point: the best setting measured on the slab workload
-DEFAULT = {"electron_tsteps": 1, "tail_boost": 32, "inflight": 1 << 21, "block": 256, "electron_split": 0.2,
-           "electron_chsteps": 4, "drain_particles": 40000}
+DEFAULT = {"electron_tsteps": 1, "tail_boost": 32, "inflight": 1 << 21, "block": 256, "electron_split": 0.15,
+           "electron_chsteps": 3, "drain_particles": 40000}
 
 
 def _rate(eng, cfg, nhist, run_kw, repeats):

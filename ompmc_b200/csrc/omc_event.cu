@@ -836,7 +836,7 @@ static int event_prepare_t(omc_engine *e) {
     S.grid = e->sm_count * std::max(1, 2048 / S.block);
     size_grids(e, S);
     // 1 measured best on the slab workload while the queues are full (with
-    // the default electron_chsteps = 2: at most two CH steps per event)
+    // the default electron_chsteps = 3: at most three CH steps per event)
     S.tsteps = e->opt.electron_tsteps > 0 ? e->opt.electron_tsteps : 1;
     S.boost = e->opt.tail_boost > 0 ? e->opt.tail_boost : 32;
     S.inflight = e->opt.inflight > 0 ? e->opt.inflight : (1LL << 20);
