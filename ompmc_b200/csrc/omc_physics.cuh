@@ -690,7 +690,7 @@ OMC_HD void roulette(const DevData<R> &D, Env &g, Part<R> &q) {
 // Annihilation at rest: two back-to-back photons of m each; p becomes the
 // first and the second is pushed (rannih, ompmc.c:4129-4185).
 template <typename R, typename Env>
-OMC_COLD void rannih(const DevData<R> &D, Env &g, Part<R> &p) {
+OMC_HD void rannih(const DevData<R> &D, Env &g, Part<R> &p) {
     R rnno = g.uni();
     R costhe = R(2) * rnno - R(1);
     R sinthe = m_sqrt(m_max(R(0), (R(1) - costhe) * (R(1) + costhe)));
@@ -960,8 +960,8 @@ struct SpinIdx {
 // (spinRejection, ompmc.c:3115-3185).  Indices are clamped to the table
 // (the reference reads one element past a row at the edges).
 template <typename R, typename Env>
-OMC_OUTLINE R spin_rej(const DevData<R> &D, Env &g, int imed, int qel, R elke, R beta2, R q1, R cost,
-                  bool &spin_index, bool is_single, SpinIdx &si) {
+OMC_HD R spin_rej(const DevData<R> &D, Env &g, int imed, int qel, R elke, R beta2, R q1, R cost, bool &spin_index,
+                  bool is_single, SpinIdx &si) {
     if (spin_index) {
         spin_index = false;
         R ai;
@@ -1018,8 +1018,8 @@ struct MsIdx {
 // surface's in-bin slope du is ums[k]-ums[k] (zero), so u is one of the 32
 // nodes; ref_compat = 0 uses ums[k+1]-ums[k].
 template <typename R, typename Env>
-OMC_OUTLINE void mscat(const DevData<R> &D, Env &g, int imed, int qel, bool &spin_index, bool &find_index, R elke,
-                  R beta2, R q1, R lambda, R chia2, R &cost, R &sint, MsIdx &mi, R &omega2, SpinIdx &si) {
+OMC_HD void mscat(const DevData<R> &D, Env &g, int imed, int qel, bool &spin_index, bool &find_index, R elke, R beta2,
+                  R q1, R lambda, R chia2, R &cost, R &sint, MsIdx &mi, R &omega2, SpinIdx &si) {
     R explambda = m_exp(-lambda);
     if (lambda <= R(13.8)) {
         R sprob = g.uni();
@@ -1144,7 +1144,7 @@ OMC_OUTLINE void mscat(const DevData<R> &D, Env &g, int imed, int qel, bool &spi
 
 // Single elastic scattering with spin rejection (sscat, ompmc.c:3188-3217).
 template <typename R, typename Env>
-OMC_COLD void sscat(const DevData<R> &D, Env &g, int imed, int qel, R chia2, R elke, R beta2, R &cost, R &sint) {
+OMC_HD void sscat(const DevData<R> &D, Env &g, int imed, int qel, R chia2, R elke, R beta2, R &cost, R &sint) {
     bool spin_index = true;
     SpinIdx si{0, 0};
     R xi, rejf, rnno;
@@ -1203,11 +1203,21 @@ OMC_HD R msdist(const DevData<R> &D, Env &g, const Part<R> &p, int imed, int iq,
     MsIdx mi{0, 0};
     SpinIdx si{0, 0};
     R omega2 = 0;
-    R w1, sint1, w2, sint2, cphi1, sphi1, cphi2, sphi2;
-    mscat(D, g, imed, qel, spin_index, find_index, elke, beta2, xi, lambda, chia2, w1, sint1, mi, omega2, si);
-    azimuth(g, cphi1, sphi1);
-    mscat(D, g, imed, qel, spin_index, find_index, elke, beta2, xi, lambda, chia2, w2, sint2, mi, omega2, si);
-    azimuth(g, cphi2, sphi2);
+    R w1 = 0, sint1 = 0, w2 = 0, sint2 = 0, cphi1 = 0, sphi1 = 0, cphi2 = 0, sphi2 = 0;
+    // the two sub-steps' deflections in that order, from one inlined copy
+    // of mscat (the results are picked by name, not by a dynamic index,
+    // so they stay in registers)
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        R w, st, cp, sp;
+        mscat(D, g, imed, qel, spin_index, find_index, elke, beta2, xi, lambda, chia2, w, st, mi, omega2, si);
+        azimuth(g, cp, sp);
+        if (k == 0) {
+            w1 = w; sint1 = st; cphi1 = cp; sphi1 = sp;
+        } else {
+            w2 = w; sint2 = st; cphi2 = cp; sphi2 = sp;
+        }
+    }
     R u2 = sint2 * cphi2, v2 = sint2 * sphi2;
     R u2p = w1 * u2 + sint1 * w2;
     R us = u2p * cphi1 - v2 * sphi1;
@@ -1313,20 +1323,7 @@ OMC_OUTLINE R eloss(const DevData<R> &D, int imed, int qel, R rhof, R tustep, R 
 }
 
 // ------------------------------------------------------- electron step
-enum EStep : int { E_DEAD = 0, E_ALIVE = 1, E_INTERACT = 2 };
-
-// Electron/positron below its cut-off: deposit the kinetic energy; a
-// positron annihilates at rest (ompmc.c:4683-4705 and repeats).
-template <typename R, typename Env>
-OMC_COLD int e_cutoff(const DevData<R> &D, Env &g, Part<R> &p, R eie) {
-    R edep = p.e - R(D_RM);
-    g.deposit(p.ir, p.wt * edep);
-    if (p.iq > 0 && edep < eie) {
-        rannih(D, g, p);
-        return E_ALIVE;
-    }
-    return E_DEAD;
-}
+enum EStep : int { E_DEAD = 0, E_ALIVE = 1, E_INTERACT = 2, E_END = 3 };
 
 // The discrete interaction at the end of electron()'s transport loop
 // (ompmc.c:5300-5451): bremsstrahlung or Moller (e-), bremsstrahlung,
@@ -1371,14 +1368,16 @@ OMC_HD void electron_interact(const DevData<R> &D, Env &g, Part<R> &p) {
     electron_interact_at(D, g, p, imed, (1 + p.iq) / 2, elke, lelke);
 }
 
-// One call of electron(): class II condensed-history transport with the
+// Class II condensed-history transport of one electron() call with the
 // fictitious cross-section method until the next discrete interaction, the
-// cut-off or the phantom exit; then the interaction (electron,
-// ompmc.c:4666-5451).  Returns E_ALIVE when p (possibly changed into another
-// particle) stays on the stack; with DEFER, E_INTERACT when p stands at its
-// discrete interaction (electron_interact samples it).
-template <typename R, typename Env, bool DEFER = false>
-OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
+// cut-off or the phantom exit (electron, ompmc.c:4666-5451).  Returns
+// E_END with the energy to deposit where the particle stands (cut-off: its
+// kinetic energy, ompmc.c:4683-4705 and repeats; phantom exit: the
+// reference's discard deposit), E_DEAD, E_ALIVE after the interaction, or
+// with DEFER E_INTERACT when p stands at its discrete interaction.  Every
+// cut-off site leaves p.e equal to the energy the reference tests (eie).
+template <typename R, typename Env, bool DEFER>
+OMC_HD int electron_transport(const DevData<R> &D, Env &g, Part<R> &p, R &edep_end) {
     const R RMr = R(D_RM);
     int irl = p.ir;
     int imed = D.med[irl];
@@ -1387,7 +1386,10 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
     int iq = p.iq;
     int qel = (1 + iq) / 2;
     int medold = imed;
-    if (eie <= ecut_of(D, irl)) return e_cutoff(D, g, p, eie);
+    if (eie <= ecut_of(D, irl)) {
+        edep_end = p.e - RMr;
+        return E_END;
+    }
 
     R elke = 0;
     int lelke = 0;
@@ -1540,13 +1542,8 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
             int irold = p.ir, irnew = p.ir, idisc = 0;
             if (call_howfar) howfar(D, p, idisc, irnew, ustep);
             if (idisc > 0) {
-                R edep = iq > 0 ? p.e + RMr : p.e - RMr;
-                g.deposit(p.ir, p.wt * edep);
-                if (iq > 0 && edep < eie) {
-                    rannih(D, g, p);
-                    return E_ALIVE;
-                }
-                return E_DEAD;
+                edep_end = iq > 0 ? p.e + RMr : p.e - RMr;
+                return E_END;
             }
             if (ustep < R(0)) ustep = R(0);
             if (ustep == R(0) || imed == -1) {
@@ -1562,7 +1559,10 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
                     imed = D.med[irl];
                     g.cross();
                 }
-                if (eie <= ecut_of(D, irl)) return e_cutoff(D, g, p, eie);
+                if (eie <= ecut_of(D, irl)) {
+                    edep_end = p.e - RMr;
+                    return E_END;
+                }
                 break;
             }
             R vstep = ustep;
@@ -1611,7 +1611,10 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
             irold = p.ir;
             eie -= edep;
             p.e = eie;
-            if (irnew == irl && eie <= ecut_of(D, irl)) return e_cutoff(D, g, p, eie);
+            if (irnew == irl && eie <= ecut_of(D, irl)) {
+                edep_end = p.e - RMr;
+                return E_END;
+            }
             medold = imed;
             if (imed != -1) {
                 const MedS<R> &M = D.ms[imed];
@@ -1625,7 +1628,10 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
                 imed = D.med[irl];
                 g.cross();
             }
-            if (eie <= ecut_of(D, irl)) return e_cutoff(D, g, p, eie);
+            if (eie <= ecut_of(D, irl)) {
+                edep_end = p.e - RMr;
+                return E_END;
+            }
             if (imed != medold) break;
             demfp -= de * sig0;
             total_de -= de;
@@ -1646,6 +1652,26 @@ OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
     if (DEFER) return E_INTERACT;
     electron_interact_at(D, g, p, imed, qel, elke, lelke);
     return E_ALIVE;
+}
+
+// One call of electron(): the transport above, then the local deposit where
+// it ends (a positron annihilates at rest there when the deposit is below
+// its energy, ompmc.c:4683-4705).  One deposit site and no call that takes
+// the particle's or the environment's address: both stay in registers in
+// the transport kernels.  Returns E_ALIVE when p (possibly changed into
+// another particle) stays on the stack; with DEFER, E_INTERACT when p
+// stands at its discrete interaction (electron_interact samples it).
+template <typename R, typename Env, bool DEFER = false>
+OMC_HD int electron_step(const DevData<R> &D, Env &g, Part<R> &p) {
+    R edep = 0;
+    const int r = electron_transport<R, Env, DEFER>(D, g, p, edep);
+    if (r != E_END) return r;
+    g.deposit(p.ir, p.wt * edep);
+    if (p.iq > 0 && edep < p.e) {
+        rannih(D, g, p);
+        return E_ALIVE;
+    }
+    return E_DEAD;
 }
 
 }  // namespace omc

@@ -49,6 +49,14 @@ OMC_HD uint64_t mix64(uint64_t z) {
 OMC_HD double u01d(uint32_t x) { return ((double)x + 0.5) * 2.3283064365386963e-10; }
 OMC_HD float u01f(uint32_t x) { return ((float)(x >> 9) + 0.5f) * 1.1920928955078125e-07f; }
 
+// One block of a stream.  One out-of-line copy instead of one per draw
+// site keeps the transport kernels small; its arguments and result travel
+// by value, so the stream's state stays in registers (an out-of-line member
+// function would take the state's address and keep it in local memory).
+__host__ __device__ __noinline__ inline U4 philox_block(uint32_t ctr, uint32_t seedw, uint32_t k0, uint32_t k1) {
+    return philox4x32_10(U4{ctr, seedw, 0x6f6d6321u, 0u}, k0, k1);
+}
+
 // A stream with a 4-number buffer.  `ctr` counts blocks consumed.
 template <typename R>
 struct Philox {
@@ -73,10 +81,9 @@ struct Philox {
     }
     // Numbers drawn so far (the argument init() resumes from).
     OMC_HD uint32_t position() const { return (ctr << 2) - 4u + (uint32_t)pos; }
-    // The block generator runs once per four numbers; one out-of-line copy
-    // instead of one per draw site keeps the transport kernels small.
-    __host__ __device__ __noinline__ void refill() {
-        buf = philox4x32_10(U4{ctr, seedw, 0x6f6d6321u, 0u}, k0, k1);
+    // The block generator runs once per four numbers.
+    OMC_HD void refill() {
+        buf = philox_block(ctr, seedw, k0, k1);
         ctr++;
         pos = 0;
     }
