@@ -102,7 +102,7 @@ typedef struct {
     double electron_split; /* event form: electrons above this kinetic energy
                              (MeV) are queued apart from the others so that
                              warps see particles of one kind (0 = one group,
-                             default 0.15); results do not depend on it */
+                             the default); results do not depend on it */
     int electron_chsteps; /* event form: condensed-history steps after which an
                              electron's distance to its next discrete
                              interaction is drawn afresh (memoryless, so the

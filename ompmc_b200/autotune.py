@@ -40,7 +40,7 @@ SPACE = {
     "drain_particles": [-1, 10000, 20000, 40000, 80000],
 }
 # the starting point: the best setting measured on the slab workload
-DEFAULT = {"electron_tsteps": 1, "tail_boost": 32, "inflight": 1 << 21, "block": 256, "electron_split": 0.15,
+DEFAULT = {"electron_tsteps": 1, "tail_boost": 32, "inflight": 1 << 21, "block": 256, "electron_split": 0.0,
            "electron_chsteps": 3, "drain_particles": 40000}
 
 

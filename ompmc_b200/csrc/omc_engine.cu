@@ -512,7 +512,7 @@ void omc_options_default(omc_options *o) {
     o->queue_capacity = 0;
     o->block = 0;
     o->nsplit = 1;
-    o->electron_split = 0.15;
+    o->electron_split = 0.0;
     o->electron_chsteps = 3;
     o->electron_interact_kernel = 1;
     o->photon_woodcock = 1;

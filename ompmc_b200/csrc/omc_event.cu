@@ -239,12 +239,16 @@ __device__ __forceinline__ int queue_index(const Q &q, int f) {
 // event's secondaries.  All 32 lanes of the warp take part (lanes without a
 // particle pass alive = false, nout = 0).  The survivor keeps its splitting
 // state (sp, sr); secondaries start unsplit.  Photons of zero weight (lost
-// a Russian roulette) would deposit nothing and are not queued.  Returns
-// the particles this lane queued.
+// a Russian roulette) would deposit nothing and are not queued, and an
+// electron at or below its region's cut-off is not queued either: its
+// first event would only deposit its kinetic energy where it stands (the
+// entry test of electron_step, which the drain applies to the same
+// particle), so that deposit is made here.  It draws no random number, so
+// trajectories do not change.  Returns the particles this lane queued.
 template <int MAXOUT, bool DEFER = false, typename R = float>
-__device__ __forceinline__ int emit(const QueueT<R> &outP, const QueueT<R> &outE, bool alive, const Part<R> &p,
-                                    EvEnv<MAXOUT, R> &g, int slot, uint32_t k0, uint32_t k1, float esplit,
-                                    int sp = -1, float sr = 0.f, const QueueT<R> *outI = nullptr,
+__device__ __forceinline__ int emit(const DevData<R> &D, const QueueT<R> &outP, const QueueT<R> &outE, bool alive,
+                                    const Part<R> &p, EvEnv<MAXOUT, R> &g, int slot, uint32_t k0, uint32_t k1,
+                                    float esplit, int sp = -1, float sr = 0.f, const QueueT<R> *outI = nullptr,
                                     bool defer = false) {
     const unsigned full = 0xffffffffu;
     uint64_t pkey = ((uint64_t)k1 << 32) | k0;
@@ -278,6 +282,10 @@ __device__ __forceinline__ int emit(const QueueT<R> &outP, const QueueT<R> &outE
         const bool toi = DEFER && k == 0 && defer;
         bool isph = has && q.iq == 0 && !toi;
         bool isel = has && q.iq != 0 && !toi;
+        if (isel && q.iq < 0 && q.e <= ecut_of(D, q.ir)) {
+            g.deposit(q.ir, q.wt * (q.e - R(D_RM)));
+            isel = false;
+        }
         int ip = warp_append(outP, isph, false, full, g.flags);
         int ie = warp_append(outE, isel, esplit > 0.f && q.e > (R)esplit, full, g.flags);
         if (ip >= 0) qstore(outP, ip, q, slot, a0, a1, ac, k == 0 ? sp : -1, k == 0 ? sr : 0.f);
@@ -289,6 +297,7 @@ __device__ __forceinline__ int emit(const QueueT<R> &outP, const QueueT<R> &outE
             queued += ii >= 0;
         }
     }
+    g.flush();
     return queued;
 }
 
@@ -443,8 +452,8 @@ __device__ __forceinline__ void transport_events(const DevData<R> &D, const Queu
             g.flush();
         }
         int emitted = KIND == EV_ELECTRON_DEFER
-                          ? emit<MAXOUT, true, R>(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr, &qi, defer)
-                          : emit<MAXOUT, false, R>(outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr);
+                          ? emit<MAXOUT, true, R>(D, outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr, &qi, defer)
+                          : emit<MAXOUT, false, R>(D, outP, outE, alive, p, g, slot, k0, k1, esplit, sp, sr);
         if (sd) add_live(sd->live, nbmax, valid ? slot : 0, valid ? emitted - 1 : 0, full);
         flags |= g.flags;
         c_ev += valid;
