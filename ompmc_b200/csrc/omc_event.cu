@@ -438,7 +438,7 @@ __device__ __forceinline__ void transport_events(const DevData<R> &D, const Queu
         bool alive = false, defer = false;
         if (valid) {
             if (KIND == EV_PHOTON) {
-                alive = photon_event(D, g, p);
+                alive = D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p);
             } else if (ELECTRON) {
                 int r = electron_step<R, EvEnv<MAXOUT, R>, KIND == EV_ELECTRON_DEFER>(D, g, p);
                 alive = r != E_DEAD;
@@ -594,7 +594,7 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<R> D, QueueT<R
             bool alive;
             if (kind == 1) alive = electron_step<R, EvEnv<MAXOUT, R>, false>(D, g, p) == E_ALIVE;
             else if constexpr (SPLIT) alive = split_event(D, g, p, sp, sr);
-            else alive = photon_event(D, g, p);
+            else alive = D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p);
             c_ev[kind]++;
             x_steps += g.work;
             c_steps[kind] += g.work;

@@ -566,31 +566,11 @@ OMC_HD void photon_interact(const DevData<R> &D, Env &g, Part<R> &p, R eig, R gl
     }
 }
 
-// A photon at its interaction site: energy, its log, the site's medium,
-// energy bin and coherent fraction.
-template <typename R>
-struct PhotonSite {
-    R eig, gle, cohfac;
-    int imed, lgle;
-};
-
-// The interaction of a photon at its site: Rayleigh by the coherent
-// fraction, else photon_interact (ompmc.c:2040-2085).
+// One call of photon(): cut-off check, number of mean free paths, voxel
+// walk to the interaction site and the interaction (photon, ompmc.c:1867-2139
+// with nsplit = 1).  Returns false when the photon is gone.
 template <typename R, typename Env>
-OMC_HD void photon_at_site(const DevData<R> &D, Env &g, Part<R> &p, const PhotonSite<R> &st) {
-    R rnno = g.uni();
-    if (rnno <= R(1) - st.cohfac) {
-        rayleigh(D, g, p, st.imed, st.gle, st.lgle);
-        return;
-    }
-    photon_interact(D, g, p, st.eig, st.gle, st.imed, st.lgle);
-}
-
-// Cut-off check, number of mean free paths and voxel walk to the site of
-// the next interaction (photon, ompmc.c:1867-2037 with nsplit = 1).
-// Returns false when the photon is gone.
-template <typename R, typename Env>
-OMC_HD bool photon_site_walk(const DevData<R> &D, Env &g, Part<R> &p, PhotonSite<R> &st) {
+OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
     R eig = p.e;
     int irl = p.ir;
     if (eig <= pcut_of(D, irl) || p.wt == R(0)) {
@@ -603,18 +583,15 @@ OMC_HD bool photon_site_walk(const DevData<R> &D, Env &g, Part<R> &p, PhotonSite
     R eta_prime = (R(1) - rnno + R(1)) - R(1);
     (void)g.uni();
     R dpmfp = -m_log(eta_prime);
-    st.eig = eig;
-    st.gle = gle;
-    return photon_walk(D, g, p, gle, dpmfp, st.imed, st.lgle, st.cohfac);
-}
-
-// One call of photon(): the walk to the site and the interaction (photon,
-// ompmc.c:1867-2139 with nsplit = 1).  Returns false when the photon is gone.
-template <typename R, typename Env>
-OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
-    PhotonSite<R> st;
-    if (!photon_site_walk(D, g, p, st)) return false;
-    photon_at_site(D, g, p, st);
+    int imed, lgle;
+    R cohfac;
+    if (!photon_walk(D, g, p, gle, dpmfp, imed, lgle, cohfac)) return false;
+    rnno = g.uni();
+    if (rnno <= R(1) - cohfac) {
+        rayleigh(D, g, p, imed, gle, lgle);
+        return true;
+    }
+    photon_interact(D, g, p, eig, gle, imed, lgle);
     return true;
 }
 
@@ -626,10 +603,9 @@ OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
 // tentative steps of -ln(xi)/mu_max, each accepted as a real interaction
 // with probability mu(x)/mu_max (a standard, exact method; Woodcock et
 // al. 1965).  A photon in a 0.25 cm grid then takes a few steps per event
-// instead of one per voxel crossed.  Leaves p at the site of the next real
-// interaction (photon_at_site samples it); returns false when it is gone.
+// instead of one per voxel crossed.  The interaction itself is photon_step's.
 template <typename R, typename Env>
-OMC_HD bool photon_site_delta(const DevData<R> &D, Env &g, Part<R> &p, PhotonSite<R> &st) {
+OMC_HD bool photon_step_delta(const DevData<R> &D, Env &g, Part<R> &p) {
     R eig = p.e;
     if (eig <= pcut_of(D, p.ir) || p.wt == R(0)) {
         g.deposit(p.ir, p.wt * eig);
@@ -686,19 +662,13 @@ OMC_HD bool photon_site_delta(const DevData<R> &D, Env &g, Part<R> &p, PhotonSit
             break;
         }
     }
-    st = PhotonSite<R>{eig, gle, cohfac, imed, lgle};
+    R rnno = g.uni();
+    if (rnno <= R(1) - cohfac) {
+        rayleigh(D, g, p, imed, gle, lgle);
+        return true;
+    }
+    photon_interact(D, g, p, eig, gle, imed, lgle);
     return true;
-}
-
-// A photon event of the event form: delta tracking on uniform grids
-// (D.woodcock) or the voxel walk to the site, then the interaction, from one
-// site of each sampler.  Returns false when the photon is gone.
-template <typename R, typename Env>
-OMC_HD bool photon_event(const DevData<R> &D, Env &g, Part<R> &p) {
-    PhotonSite<R> st;
-    const bool at = D.woodcock ? photon_site_delta(D, g, p, st) : photon_site_walk(D, g, p, st);
-    if (at) photon_at_site(D, g, p, st);
-    return at;
 }
 
 // Russian roulette of a photon made by an electron interaction when photons
