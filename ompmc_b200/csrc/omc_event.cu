@@ -109,7 +109,9 @@ struct EvEnv {
     }
     __device__ void cross() { ncross++; }
     __device__ bool tstep_take() { return tleft-- > 0; }
-    __device__ bool push(const Part<R> &q) {
+    __device__ bool push(const Part<R> &q) { return push_at(q, rng.position()); }
+    // A push made at stream position `pos` (an event run out of line).
+    __device__ bool push_at(const Part<R> &q, uint32_t pos) {
         if (nout >= MAXOUT) {
             flags |= ERR_STACK;
             return false;
@@ -118,7 +120,7 @@ struct EvEnv {
 #pragma unroll
         for (int k = 0; k < MAXOUT; k++)
             if (k == nout) {
-                out_pos[k] = rng.position();
+                out_pos[k] = pos;
                 out[k] = q;
             }
         nout++;
@@ -127,6 +129,22 @@ struct EvEnv {
     __device__ void err(unsigned f) { flags |= f; }
     __device__ bool tick() { return ++work < EV_BUDGET; }
 };
+
+// A photon event through the out-of-line photon_event_outline: its results
+// folded back into the event environment in the order the photon step
+// itself would have made them (stream, counters, deposit, pushed product).
+template <int MAXOUT, typename R>
+__device__ __forceinline__ bool photon_event(const DevData<R> &D, EvEnv<MAXOUT, R> &g, Part<R> &p) {
+    const PhotonEventOut<R> o = photon_event_outline<R>(D, p, g.rng, g.work, EV_BUDGET);
+    p = o.p;
+    g.rng = o.e.rng;
+    g.work = o.e.work;
+    g.ncross += o.e.ncross;
+    g.flags |= o.e.flags;
+    if (o.e.dep_ir >= 0) g.deposit(o.e.dep_ir, o.e.dep_e);
+    if (o.e.nq) g.push_at(o.e.q, o.e.qpos);
+    return o.alive != 0;
+}
 
 template <typename R = float>
 struct SrcEnv {
@@ -438,7 +456,7 @@ __device__ __forceinline__ void transport_events(const DevData<R> &D, const Queu
         bool alive = false, defer = false;
         if (valid) {
             if (KIND == EV_PHOTON) {
-                alive = D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p);
+                alive = photon_event(D, g, p);
             } else if (ELECTRON) {
                 int r = electron_step<R, EvEnv<MAXOUT, R>, KIND == EV_ELECTRON_DEFER>(D, g, p);
                 alive = r != E_DEAD;
@@ -594,7 +612,7 @@ __global__ void __launch_bounds__(DRAIN_BLOCK, 4) k_drain(DevData<R> D, QueueT<R
             bool alive;
             if (kind == 1) alive = electron_step<R, EvEnv<MAXOUT, R>, false>(D, g, p) == E_ALIVE;
             else if constexpr (SPLIT) alive = split_event(D, g, p, sp, sr);
-            else alive = D.woodcock ? photon_step_delta(D, g, p) : photon_step(D, g, p);
+            else alive = photon_event(D, g, p);
             c_ev[kind]++;
             x_steps += g.work;
             c_steps[kind] += g.work;

@@ -239,7 +239,7 @@ OMC_HD Part<R> uphi32(const Part<R> &p, const Uphi<R> &h, R costhe, R sinthe) {
 // `(int)rnno0*dwi` == 0 and the form-factor tables of medium 0 are used
 // for every medium.
 template <typename R, typename Env>
-OMC_COLD void rayleigh(const DevData<R> &D, Env &g, Part<R> &p, int imed, R gle, int lgle) {
+OMC_HD void rayleigh_body(const DevData<R> &D, Env &g, Part<R> &p, int imed, R gle, int lgle) {
     R eig = p.e;
     R pmax = pwl(D.pmax[imed * D_MXGE + (lgle < 0 ? 0 : (lgle > D_MXGE - 1 ? D_MXGE - 1 : lgle))], gle);
     R xmax = R(80.65506856998) * eig;
@@ -269,6 +269,13 @@ OMC_COLD void rayleigh(const DevData<R> &D, Env &g, Part<R> &p, int imed, R gle,
     uphi21(g, p, h, costhe, sinthe);
 }
 
+// Out-of-line copy (the plain form, the split photons and the electron
+// kernels call it by reference).
+template <typename R, typename Env>
+OMC_COLD void rayleigh(const DevData<R> &D, Env &g, Part<R> &p, int imed, R gle, int lgle) {
+    rayleigh_body(D, g, p, imed, gle, lgle);
+}
+
 // Pair rejection function in xi (PIRS-0287 eq. 4; ompmc.c:1436-1445).
 template <typename R>
 OMC_HD R pair_rej(R zbrang, R xi, R esedei, R eseder, R tteig) {
@@ -283,7 +290,7 @@ OMC_HD R pair_rej(R zbrang, R xi, R esedei, R eseder, R tteig) {
 // p becomes particle 1 and particle 2 is pushed.  quirk: the angle loop
 // accepts as soon as theta < pi.
 template <typename R, typename Env>
-OMC_COLD void pair(const DevData<R> &D, Env &g, Part<R> &p, int imed) {
+OMC_HD void pair_body(const DevData<R> &D, Env &g, Part<R> &p, int imed) {
     const MedS<R> &M = D.ms[imed];
     const R RMr = R(D_RM);
     R eig = p.e, ese1, ese2;
@@ -390,10 +397,17 @@ OMC_COLD void pair(const DevData<R> &D, Env &g, Part<R> &p, int imed) {
     g.push(q);
 }
 
+// Out-of-line copy (the plain form, the split photons and the electron
+// kernels call it by reference).
+template <typename R, typename Env>
+OMC_COLD void pair(const DevData<R> &D, Env &g, Part<R> &p, int imed) {
+    pair_body(D, g, p, imed);
+}
+
 // Compton scattering off free electrons, Klein-Nishina (compton,
 // ompmc.c:1688-1801).  p stays the scattered photon; the electron is pushed.
 template <typename R, typename Env>
-OMC_COLD void compton(const DevData<R> &D, Env &g, Part<R> &p) {
+OMC_HD void compton_body(const DevData<R> &D, Env &g, Part<R> &p) {
     const R RMr = R(D_RM);
     R eig = p.e, ko = p.e / RMr;
     R broi = R(1) + R(2) * ko, bro = R(1) / broi;
@@ -457,11 +471,18 @@ OMC_COLD void compton(const DevData<R> &D, Env &g, Part<R> &p) {
     g.push(q);
 }
 
+// Out-of-line copy (the plain form, the split photons and the electron
+// kernels call it by reference).
+template <typename R, typename Env>
+OMC_COLD void compton(const DevData<R> &D, Env &g, Part<R> &p) {
+    compton_body(D, g, p);
+}
+
 // Photo-absorption: the photon becomes an electron with E + m, emitted
 // along the Sauter distribution when above the region's cut-off
 // (photo, ompmc.c:1804-1864).
 template <typename R, typename Env>
-OMC_COLD void photo(const DevData<R> &D, Env &g, Part<R> &p) {
+OMC_HD void photo_body(const DevData<R> &D, Env &g, Part<R> &p) {
     const R RMr = R(D_RM);
     p.e += RMr;
     p.iq = -1;
@@ -498,6 +519,45 @@ OMC_COLD void photo(const DevData<R> &D, Env &g, Part<R> &p) {
         Uphi<R> h;
         uphi21(g, p, h, costhe, sinthe);
     }
+}
+
+// Out-of-line copy (the plain form, the split photons and the electron
+// kernels call it by reference).
+template <typename R, typename Env>
+OMC_COLD void photo(const DevData<R> &D, Env &g, Part<R> &p) {
+    photo_body(D, g, p);
+}
+
+// Environments that declare kInlineSamplers = true (the out-of-line photon
+// event of the event form) get the photon samplers inlined; every other
+// caller uses their out-of-line copies.
+template <typename Env, typename = void>
+struct InlineSamplers {
+    static constexpr bool value = false;
+};
+template <typename Env>
+struct InlineSamplers<Env, decltype((void)Env::kInlineSamplers)> {
+    static constexpr bool value = Env::kInlineSamplers;
+};
+template <typename R, typename Env>
+OMC_HD void rayleigh_at(const DevData<R> &D, Env &g, Part<R> &p, int imed, R gle, int lgle) {
+    if constexpr (InlineSamplers<Env>::value) rayleigh_body(D, g, p, imed, gle, lgle);
+    else rayleigh(D, g, p, imed, gle, lgle);
+}
+template <typename R, typename Env>
+OMC_HD void pair_at(const DevData<R> &D, Env &g, Part<R> &p, int imed) {
+    if constexpr (InlineSamplers<Env>::value) pair_body(D, g, p, imed);
+    else pair(D, g, p, imed);
+}
+template <typename R, typename Env>
+OMC_HD void compton_at(const DevData<R> &D, Env &g, Part<R> &p) {
+    if constexpr (InlineSamplers<Env>::value) compton_body(D, g, p);
+    else compton(D, g, p);
+}
+template <typename R, typename Env>
+OMC_HD void photo_at(const DevData<R> &D, Env &g, Part<R> &p) {
+    if constexpr (InlineSamplers<Env>::value) photo_body(D, g, p);
+    else photo(D, g, p);
 }
 
 // --------------------------------------------------------- photon step
@@ -558,11 +618,11 @@ OMC_HD void photon_interact(const DevData<R> &D, Env &g, Part<R> &p, R eig, R gl
     const PhBin<R> &b = pbin(D, imed, lgle);
     R gbr1 = pwl(b.gbr1, gle);
     if (rnno <= gbr1 && eig > R(2) * R(D_RM)) {
-        pair(D, g, p, imed);
+        pair_at(D, g, p, imed);
     } else {
         R gbr2 = pwl(b.gbr2, gle);
-        if (rnno < gbr2) compton(D, g, p);
-        else photo(D, g, p);
+        if (rnno < gbr2) compton_at(D, g, p);
+        else photo_at(D, g, p);
     }
 }
 
@@ -588,7 +648,7 @@ OMC_HD bool photon_step(const DevData<R> &D, Env &g, Part<R> &p) {
     if (!photon_walk(D, g, p, gle, dpmfp, imed, lgle, cohfac)) return false;
     rnno = g.uni();
     if (rnno <= R(1) - cohfac) {
-        rayleigh(D, g, p, imed, gle, lgle);
+        rayleigh_at(D, g, p, imed, gle, lgle);
         return true;
     }
     photon_interact(D, g, p, eig, gle, imed, lgle);
@@ -664,11 +724,80 @@ OMC_HD bool photon_step_delta(const DevData<R> &D, Env &g, Part<R> &p) {
     }
     R rnno = g.uni();
     if (rnno <= R(1) - cohfac) {
-        rayleigh(D, g, p, imed, gle, lgle);
+        rayleigh_at(D, g, p, imed, gle, lgle);
         return true;
     }
     photon_interact(D, g, p, eig, gle, imed, lgle);
     return true;
+}
+
+// ------------------------------------------ the out-of-line photon event
+// The environment of a photon event run out of line (the event form): the
+// photon's stream, the product it pushes (every sampler pushes at most
+// one) with the stream position at the push, its deposit (a photon event
+// deposits at most once: below the cut-off), its step and crossing counts
+// and error flags — all returned by value.
+template <typename R>
+struct PhotonEnv {
+    static constexpr bool kInlineSamplers = true;
+    Philox<R> rng;
+    Part<R> q;
+    uint32_t qpos;
+    int nq;
+    int dep_ir;
+    R dep_e;
+    int work, budget, ncross;
+    unsigned flags;
+    OMC_HD R uni() { return rng.uni(); }
+    OMC_HD bool push(const Part<R> &x) {
+        if (nq) {
+            flags |= ERR_STACK;
+            return false;
+        }
+        qpos = rng.position();
+        q = x;
+        nq = 1;
+        return true;
+    }
+    OMC_HD void err(unsigned f) { flags |= f; }
+    OMC_HD bool tick() { return ++work < budget; }
+    OMC_HD void cross() { ncross++; }
+    OMC_HD void deposit(int ir, R e) {
+        if (dep_ir >= 0 && ir != dep_ir) flags |= ERR_STACK;
+        dep_ir = ir;
+        dep_e += e;
+    }
+};
+
+template <typename R>
+struct PhotonEventOut {
+    Part<R> p;
+    PhotonEnv<R> e;
+    int alive;
+};
+
+// One photon event (delta tracking on uniform grids, else the voxel walk,
+// then the interaction) compiled once, out of line, with its inputs and
+// results by value: every kernel that runs photon events (the transport
+// cycles and the drain) runs the same machine code for them, so they
+// agree to the bit, and the calling kernel's particle and environment
+// never have their address taken.
+template <typename R>
+OMC_COLD PhotonEventOut<R> photon_event_outline(const DevData<R> &D, Part<R> p, Philox<R> rng, int work,
+                                                int budget) {
+    PhotonEventOut<R> o;
+    o.e.rng = rng;
+    o.e.qpos = 0;
+    o.e.nq = 0;
+    o.e.dep_ir = -1;
+    o.e.dep_e = R(0);
+    o.e.work = work;
+    o.e.budget = budget;
+    o.e.ncross = 0;
+    o.e.flags = 0;
+    o.alive = (D.woodcock ? photon_step_delta(D, o.e, p) : photon_step(D, o.e, p)) ? 1 : 0;
+    o.p = p;
+    return o;
 }
 
 // Russian roulette of a photon made by an electron interaction when photons
