@@ -42,9 +42,9 @@ constexpr int EV_MAXOUT_SPLIT = 2; // products of a split photon's sub-photon (p
 constexpr int EV_MAX_BLOCK = 256;  // launch bound of the transport kernels
 // Resident 256-thread blocks per SM the electron kernel is compiled for:
 // four (64 registers) in FP32, two (128 registers) in FP64.  Measured on the
-// served beamlet load and the slab beam: 4 blocks 27.5 and 45.9 M hist/s,
-// 6 blocks 27.3 and 46.1, 8 blocks (32 registers) 27.0 and 45.9, while the
-// 8-block build's spilled frames made 6x the DRAM writes of the 4-block one.
+// served beamlet load and the slab beam with the step's state in
+// registers: 3 blocks (80 registers) 50.6 and 70.3 M hist/s, 4 blocks 52.6
+// and 71.8, 5 blocks (48 registers) 52.1 and 70.3.
 template <typename R>
 constexpr int electron_minb() {
     return sizeof(R) == 4 ? 4 : 2;

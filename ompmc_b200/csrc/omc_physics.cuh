@@ -762,8 +762,9 @@ struct PhotonEnv {
     OMC_HD void err(unsigned f) { flags |= f; }
     OMC_HD bool tick() { return ++work < budget; }
     OMC_HD void cross() { ncross++; }
+    // one deposit record: a second deposit elsewhere would not fit it
     OMC_HD void deposit(int ir, R e) {
-        if (dep_ir >= 0 && ir != dep_ir) flags |= ERR_STACK;
+        if (dep_ir >= 0 && ir != dep_ir) flags |= ERR_LOG;
         dep_ir = ir;
         dep_e += e;
     }
