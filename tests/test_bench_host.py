@@ -42,3 +42,33 @@ def test_clock_record_median_and_reasons():
     r = c.stop()
     assert r["sm_mhz"] == 1965.0 and r["sm_max_mhz"] == 1965.0 and r["samples"] == 3
     assert r["reasons"] == ["sw_power_cap"]
+
+
+def test_committed_profile_figures_parse():
+    # the roofline line of the headline reads these per-event figures from
+    # the committed ncu summaries
+    req = bench.ncu_figure(bench.PROFILE_REQUESTS, "requested_bytes_per_event")
+    dram = bench.ncu_figure(bench.PROFILE_REQUESTS, "dram_bytes_per_event")
+    slab = bench.ncu_traffic_per_event()
+    assert req is not None and req > 104          # more than the queue state alone
+    assert dram is not None and 0 < dram < req + 1000
+    assert slab is not None and slab > 0
+    assert bench.ncu_figure(bench.PROFILE_REQUESTS, "no_such_key") is None
+    assert bench.ncu_figure("no_such_profile.md", "requested_bytes_per_event") is None
+
+
+def test_uncertainty_summaries():
+    # unc^2 * histories is the per-history relative variance; histories for
+    # 1 % divide it by 1e-4; non-finite columns are left out
+    unc = np.array([0.1, 0.2, np.nan])
+    nh = np.array([1e4, 2.5e3, 1e3])
+    s = bench.unc_summary(unc, nh, 1e6)
+    assert s["beamlets"] == 2
+    assert np.isclose(s["rel_var_x_histories"], 100.0)
+    assert np.isclose(s["histories_to_1pct_per_beamlet"], 1e6)
+    assert np.isclose(s["seconds_to_1pct_per_beamlet"], 1.0)
+    assert np.isclose(s["mean_rel_unc_gt50pct_dmax"], 0.15)
+    res = [{"nhist": 1e4, "loop_s": 0.5, "unc": 0.1}, {"nhist": 3e4, "loop_s": 1.5, "unc": 0.1}]
+    r = bench.ref_summary(res)
+    assert np.isclose(r["value"], 2e4) and np.isclose(r["loop_s"], 2.0)
+    assert r["p50_ms"] == 1000.0 and r["unc"]["beamlets"] == 2
