@@ -77,10 +77,36 @@ struct Rayl {
     int ia[D_MXRAYFF];
 };
 
+// Division of a non-negative 32-bit integer n < 2^31 by a run-time
+// constant d >= 1 with a multiply-high, an add and a shift (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", PLDI
+// 1994): with s = ceil(log2 d) and M = floor(2^(32+s) / d) + 1 < 2^33,
+// n / d = floor(n M / 2^(32+s)) exactly for every n < 2^32; M = 2^32 + m
+// with m < 2^32 gives n / d = (mulhi(n, m) + n) >> s, and the sum stays
+// below 2^32 for n < 2^31.  The GPU has no integer divide instruction.
+struct FastDiv {
+    uint32_t d, m, s;
+    static FastDiv make(uint32_t d) {
+        FastDiv f{d, 0u, 0u};
+        while ((1ull << f.s) < d) f.s++;
+        f.m = (uint32_t)(((1ull << (32 + f.s)) / d + 1) - (1ull << 32));
+        return f;
+    }
+    __host__ __device__ __forceinline__ uint32_t div(uint32_t n) const {
+#ifdef __CUDA_ARCH__
+        const uint32_t hi = __umulhi(n, m);
+#else
+        const uint32_t hi = (uint32_t)(((uint64_t)n * m) >> 32);
+#endif
+        return (hi + n) >> s;
+    }
+};
+
 template <typename R>
 struct DevData {
     int nmed;
     int nx, ny, nz;
+    FastDiv div_nx, div_nxy;         // n / nx and n / (nx*ny) for region indices
     const R *xb, *yb, *zb;          // voxel boundaries
     const int8_t *med;               // [nvox+1] medium index per region, -1 = vacuum / outside
     const R *rhof;                   // [nvox+1] density / PEGS density

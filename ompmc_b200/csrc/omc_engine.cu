@@ -80,6 +80,8 @@ void make_layout(const Tables &t, const Phantom &ph, const Regions &rg, double e
     d.nx = ph.nx;
     d.ny = ph.ny;
     d.nz = ph.nz;
+    d.div_nx = FastDiv::make((uint32_t)ph.nx);
+    d.div_nxy = FastDiv::make((uint32_t)ph.nx * (uint32_t)ph.ny);
     d.ref_compat = ref_compat;
     d.nsplit = 1;
     // uniform grid and per-medium density maxima (photon delta tracking)

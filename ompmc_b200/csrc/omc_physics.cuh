@@ -111,6 +111,20 @@ OMC_HD const PhBin<R> &pbin(const DevData<R> &D, int imed, int l) {
 }
 
 // ------------------------------------------------------------- geometry
+// Column, row and plane of region irl (1-based, x fastest): the
+// reference's (irl-1) % nx, / (nx*ny) and / nx, by exact multiply-high
+// divisions.
+template <typename R>
+OMC_HD void voxel_ijk(const DevData<R> &D, int irl, int &irx, int &iry, int &irz) {
+    const uint32_t n = (uint32_t)(irl - 1);
+    const uint32_t k = D.div_nxy.div(n);
+    const uint32_t r = n - k * D.div_nxy.d;
+    const uint32_t j = D.div_nx.div(r);
+    irx = (int)(r - j * D.div_nx.d);
+    iry = (int)j;
+    irz = (int)k;
+}
+
 // Distance to the next voxel plane along the direction, checked in the
 // order z, x, y; the new region is the neighbour across that plane or 0
 // (outside); a particle already outside is discarded
@@ -123,9 +137,8 @@ OMC_HD void howfar(const DevData<R> &D, const Part<R> &p, int &idisc, int &irnew
         return;
     }
     int imax = D.nx, ijmax = D.nx * D.ny;
-    int irx = (irl - 1) % imax;
-    int irz = (irl - 1 - irx) / ijmax;
-    int iry = ((irl - 1 - irx) - irz * ijmax) / imax;
+    int irx, iry, irz;
+    voxel_ijk(D, irl, irx, iry, irz);
     R dist;
     if (p.w > R(0)) {
         dist = (D.zb[irz + 1] - p.z) / p.w;
@@ -156,10 +169,8 @@ template <typename R>
 OMC_HD R hownear(const DevData<R> &D, const Part<R> &p) {
     int irl = p.ir;
     if (irl == 0) return R(0);
-    int imax = D.nx, ijmax = D.nx * D.ny;
-    int irx = (irl - 1) % imax;
-    int irz = (irl - 1 - irx) / ijmax;
-    int iry = ((irl - 1 - irx) - irz * ijmax) / imax;
+    int irx, iry, irz;
+    voxel_ijk(D, irl, irx, iry, irz);
     R t = R(1.0E10);
     t = m_min(t, D.xb[irx + 1] - p.x);
     t = m_min(t, p.x - D.xb[irx]);
