@@ -88,6 +88,11 @@ struct FastDiv {
     uint32_t d, m, s;
     static FastDiv make(uint32_t d) {
         FastDiv f{d, 0u, 0u};
+        if (d > (1u << 31)) {
+            // every n < 2^31 is below d: m = 0, s = 31 gives n >> 31 = 0
+            f.s = 31;
+            return f;
+        }
         while ((1ull << f.s) < d) f.s++;
         f.m = (uint32_t)(((1ull << (32 + f.s)) / d + 1) - (1ull << 32));
         return f;

@@ -20,7 +20,7 @@ int main() {
     int nd = 0;
     for (uint32_t d = 1; d <= 5000; d++) ds[nd++] = d;
     const uint32_t extra[] = {64u * 64u, 128u * 128u, 256u * 256u, 30u * 30u, 32u * 32u, 1u << 20, 65537u, 1000003u,
-                              (1u << 31) - 1u};
+                              (1u << 31) - 1u, 1u << 31, (1u << 31) + 1u, 4000000000u, 4294967295u};
     for (uint32_t d : extra) ds[nd++] = d;
     for (int a = 0; a < nd; a++) {
         const uint32_t d = ds[a];
